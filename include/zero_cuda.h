@@ -1,0 +1,128 @@
+/* zero_cuda.h -- C ABI of the B200 (sm_100a) ZB2 block codec.
+ *
+ * A drop-in for the GPU codec behind `zero c / x / t / bench`: it replaces the reference's Level Zero
+ * layer (src/ze_min.h, src/gpu.h) and its GPU orchestration (src/gpu_codec.h) with CUDA kernels behind
+ * plain C entry points.  The reference's callers reach the GPU codec through the virtual interface
+ * zero::Codec (src/archive.h:56-69); each entry point below names the method it backs.  A C++ adapter
+ * implementing zero::Codec over these calls is in include/zero_cuda_codec.hpp.
+ *
+ * Format: the .zero block format is unchanged (ZB2 payloads of src/codec2.h, rANS streams of
+ * src/codec.h, CRC-32 of src/crc32.h).  At the same level the encoder writes exactly the bytes the
+ * reference CPU codec writes (same parse: hash chains of depth 8 / 32 / 256 for levels 1 / 2-8 / 9,
+ * src/main.cpp:45, 54; one lazy step; matches up to 4096 bytes).
+ *
+ * Errors (the reference throws; here every call returns a status):
+ *   ZC_OK        success
+ *   ZC_E_DATA    damaged input or an impossible result (the reference's zb::Error: retry on the CPU,
+ *                which reports what is wrong -- src/safe_codec.h:36-49)
+ *   ZC_E_DEVICE  the GPU failed (the reference's gpu::Error: fall back to the CPU for good)
+ *   ZC_E_NOMEM   device memory could not be had
+ *   ZC_E_ARG     a bad argument (block size outside 16..20, a block longer than the block size, ...)
+ * zc_last_error(ctx) gives the message of the last failure on that context.
+ *
+ * Threading: a context is used by one host thread at a time (the reference calls its codec from one
+ * thread, src/archive.h:381-413, 599-633).  Separate contexts may run on separate threads.
+ */
+#ifndef ZERO_CUDA_H
+#define ZERO_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ZC_OK = 0, ZC_E_DATA = 1, ZC_E_DEVICE = 2, ZC_E_NOMEM = 3, ZC_E_ARG = 4 };
+
+/* block methods, as in the block record of the archive (src/archive.h:395-398) */
+enum { ZC_METHOD_STORED = 0, ZC_METHOD_ZB2 = 1 };
+
+typedef struct zc_ctx zc_ctx;
+
+/* Opens device `device` (replaces GpuCodec::open, src/gpu_codec.h:75-86, and gpu::Device::open,
+ * src/gpu.h:140-188).  No kernel compilation at run time: the kernels are built ahead for sm_100a. */
+int zc_open(zc_ctx **ctx, int device);
+void zc_close(zc_ctx *ctx);
+
+/* The message of the last error on this context ("" when none). */
+const char *zc_last_error(const zc_ctx *ctx);
+
+/* The codec's name for the user (zero::Codec::name, src/archive.h:58). */
+const char *zc_name(const zc_ctx *ctx);
+
+/* Block size and level before a job (zero::Codec::prepare, src/archive.h:68, and the level choice of
+ * src/gpu_codec.h:63-70).  block_log 16..20, level 1..9.  Optional: every call below takes both. */
+int zc_prepare(zc_ctx *ctx, uint32_t block_log, int level);
+
+/* Bytes of input one compress / decompress call should hold (zero::Codec::batch_bytes and
+ * batch_bytes_decode, src/archive.h:65-66). */
+size_t zc_batch_bytes(const zc_ctx *ctx, uint32_t block_log);
+size_t zc_batch_bytes_decode(const zc_ctx *ctx, uint32_t block_log);
+
+/* Compresses n host bytes cut into blocks of 2^block_log (the last may be shorter): zero::Codec::compress
+ * (src/archive.h:60; src/gpu_codec.h:153-229).  Per block b (nb = ceil(n / 2^block_log)):
+ *   methods[b]    ZC_METHOD_ZB2, or ZC_METHOD_STORED when the payload would not be smaller than the block
+ *   comp_lens[b]  the payload length (for a stored block: its raw length; nothing is written for it)
+ *   crcs[b]       CRC-32 of the block's raw bytes (the record's checksum, src/archive.h:376)
+ *   pay_offs[b]   where block b's payload starts in `payloads` (ZB2 payloads are packed back to back)
+ * payloads must hold payload_cap bytes; n bytes always suffice.  Any of crcs / pay_offs may be NULL. */
+int zc_compress(zc_ctx *ctx, const uint8_t *in, size_t n, uint32_t block_log, int level, uint8_t *methods,
+                uint32_t *comp_lens, uint32_t *crcs, uint8_t *payloads, size_t payload_cap, uint64_t *pay_offs);
+
+/* The same for nb blocks of uneven sizes from many files, in one launch per stage: block b is
+ * in_lens[b] (<= 2^block_log) bytes at in + in_offs[b]. */
+int zc_compress_batch(zc_ctx *ctx, const uint8_t *in, const uint64_t *in_offs, const uint32_t *in_lens, uint32_t nb,
+                      uint32_t block_log, int level, uint8_t *methods, uint32_t *comp_lens, uint32_t *crcs,
+                      uint8_t *payloads, size_t payload_cap, uint64_t *pay_offs);
+
+/* Decompresses nb blocks (zero::Codec::decompress, src/archive.h:63; src/gpu_codec.h:253-315).
+ * Block b is comp_lens[b] bytes at comp + comp_offs[b] with method methods[b] and raw length raw_lens[b].
+ * Writes the raw bytes of all blocks back to back into out (sum of raw_lens bytes).
+ * crcs_out[b] (may be NULL) gets the CRC-32 of block b's output; block_err[b] (may be NULL) a nonzero
+ * code for a damaged block.  Returns ZC_E_DATA when any block is damaged. */
+int zc_decompress(zc_ctx *ctx, const uint8_t *comp, const uint64_t *comp_offs, const uint32_t *comp_lens,
+                  const uint8_t *methods, const uint32_t *raw_lens, uint32_t nb, uint8_t *out, uint32_t *crcs_out,
+                  uint32_t *block_err);
+
+/* ---- device-resident forms: every pointer is device memory, work is queued on `stream` (a
+ * cudaStream_t; NULL for the legacy default stream) and the call returns once it is queued.  For
+ * callers that keep data on the GPU, and for measuring the kernels without host copies.
+ * d_in must be 4-byte aligned with at least 16 readable bytes after the last block (the match finder
+ * reads whole aligned words, as the reference's kernels do: kernels/zero.cl:30-31).
+ *
+ * zc_compress_device: nb blocks at d_in + d_in_offs[b], d_in_lens[b] bytes each.  Writes d_methods,
+ * d_comp_lens, d_crcs (may be NULL) and the payloads packed into d_out (out_cap bytes) at d_out_offs[b];
+ * a stored block's raw bytes are copied into d_out as well, so d_out holds every record body in order.
+ * *d_total (device u64) gets the bytes written to d_out. */
+int zc_compress_device(zc_ctx *ctx, const uint8_t *d_in, const uint64_t *d_in_offs, const uint32_t *d_in_lens,
+                       uint32_t nb, uint32_t block_log, int level, uint8_t *d_methods, uint32_t *d_comp_lens,
+                       uint32_t *d_crcs, uint8_t *d_out, size_t out_cap, uint64_t *d_out_offs, uint64_t *d_total,
+                       void *stream);
+
+/* zc_decompress_device: block b is d_comp_lens[b] bytes at d_comp + d_comp_offs[b]; its raw bytes go to
+ * d_out + d_out_offs[b].  d_crcs (may be NULL) gets each output's CRC-32, d_err each block's status.
+ * block_log bounds the raw lengths (a block longer than 2^block_log is damaged). */
+int zc_decompress_device(zc_ctx *ctx, const uint8_t *d_comp, const uint64_t *d_comp_offs, const uint32_t *d_comp_lens,
+                         const uint8_t *d_methods, const uint32_t *d_raw_lens, uint32_t nb, uint32_t block_log,
+                         uint8_t *d_out, const uint64_t *d_out_offs, uint32_t *d_crcs, uint32_t *d_err, void *stream);
+
+/* CRC-32 of host bytes on the GPU (crc32::of, src/crc32.h:51), and CRC combination on the host
+ * (crc32::combine, src/crc32.h:60-66): the CRC of A followed by B. */
+int zc_crc32(zc_ctx *ctx, const uint8_t *data, size_t n, uint32_t *crc);
+uint32_t zc_crc32_combine(uint32_t crc_a, uint32_t crc_b, uint64_t len_b);
+
+/* Kernel launches this context has issued since it was opened (for accounting). */
+uint64_t zc_launch_count(const zc_ctx *ctx);
+
+/* Per-stage timing (the reference's ZERO_PROFILE stage times, src/gpu_codec.h:32-49): with on != 0 every
+ * kernel launch is bracketed by CUDA events on its stream (no device syncs); zc_profile clears the
+ * totals.  zc_profile_stages waits for the recorded events and reports, per kernel in first-launch
+ * order, its name (names + 32*i, NUL-terminated), total milliseconds and launches; *n_out = stages. */
+int zc_profile(zc_ctx *ctx, int on);
+int zc_profile_stages(zc_ctx *ctx, uint32_t max, char *names, double *ms, uint64_t *counts, uint32_t *n_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZERO_CUDA_H */

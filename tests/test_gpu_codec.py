@@ -1,0 +1,191 @@
+"""GPU parity: the CUDA codec against the oracle (the C restatement of the reference CPU codec, pinned by the
+reference's golden vectors).  Integer work, so every comparison is bit-exact."""
+import random
+
+import numpy as np
+import pytest
+
+from conftest import block_input, block_payload, load_manifest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+LEVELS = (1, 5, 9)
+
+
+@pytest.fixture(scope="module")
+def codec():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("a CUDA device is required for -m gpu")
+    if not O.Port.available():
+        O.build()
+    import zero_cuda as Z
+    c = Z.CudaCodec(level=5)
+    yield c
+    c.close()
+
+
+def block_log_for(n):
+    bl = 16
+    while (1 << bl) < n:
+        bl += 1
+    return bl
+
+
+def cpu_blocks(data, block_log, level):
+    """The oracle's per-block (method, payload) for data cut into blocks."""
+    B = 1 << block_log
+    out = []
+    for o in range(0, len(data), B):
+        blk = data[o:o + B]
+        pay = O.Port.compress_block(blk, O.depth_for_level(level))
+        out.append((0, None) if len(pay) >= len(blk) else (1, pay))
+    return out
+
+
+def test_crc32(codec):
+    rng = random.Random(7)
+    for n in (0, 1, 7, 8, 9, 1000, 65536, 1 << 20, (1 << 20) + 13, 3 * (1 << 20) + 5):
+        d = rng.randbytes(n)
+        assert codec.crc32(d) == O.Port.crc32(d), n
+
+
+def test_decode_golden(codec, manifest):
+    for ent in manifest["blocks"]:
+        data = block_input(ent)
+        for lv in LEVELS:
+            pay = block_payload(ent, lv)
+            if pay is None:
+                continue
+            raw, crcs, errs = codec.decompress_arrays(pay, [0], [len(pay)], [1], [len(data)])
+            assert errs[0] == 0, (ent["name"], lv)
+            assert raw.tobytes() == data, (ent["name"], lv)
+            assert crcs[0] == ent["crc32"], (ent["name"], lv)
+
+
+def test_encode_golden(codec, manifest):
+    for ent in manifest["blocks"]:
+        data = block_input(ent)
+        bl = block_log_for(len(data))
+        for lv in LEVELS:
+            want = ent["levels"][str(lv)]
+            methods, lens, crcs, pay, offs = codec.compress_arrays(data, bl, level=lv)
+            assert len(methods) == 1
+            assert crcs[0] == ent["crc32"]
+            if want["stored"]:
+                assert methods[0] == 0, (ent["name"], lv)
+            else:
+                assert methods[0] == 1, (ent["name"], lv)
+                got = pay[int(offs[0]): int(offs[0]) + int(lens[0])].tobytes()
+                assert got == block_payload(ent, lv), (ent["name"], lv)
+
+
+def test_stored_block_decode(codec):
+    rng = random.Random(3)
+    d = rng.randbytes(70000)
+    raw, crcs, errs = codec.decompress_arrays(d, [0], [len(d)], [0], [len(d)])
+    assert errs[0] == 0 and raw.tobytes() == d and crcs[0] == O.Port.crc32(d)
+
+
+@pytest.mark.parametrize("block_log", [16, 18, 20])
+@pytest.mark.parametrize("level", LEVELS)
+def test_multi_block_parity(codec, block_log, level):
+    """Workload-shaped data over several blocks: payloads byte-identical to the oracle, round trip exact."""
+    import datagen as G
+    B = 1 << block_log
+    n = 3 * B + B // 3 + 17  # a short tail block
+    parts = [G.text_mix(n // 3, 100 + block_log), G.lz_mix(n // 3, block_log, 200 + level),
+             G.random_bytes(n - 2 * (n // 3), 300)]
+    data = np.concatenate(parts).tobytes()
+    methods, lens, crcs, pay, offs = codec.compress_arrays(data, block_log, level=level)
+    want = cpu_blocks(data, block_log, level)
+    assert len(methods) == len(want)
+    comp, coffs = [], []
+    at = 0
+    for b, (m, p) in enumerate(want):
+        blk = data[b * B:(b + 1) * B]
+        assert crcs[b] == O.Port.crc32(blk)
+        assert methods[b] == m, b
+        if m:
+            got = pay[int(offs[b]): int(offs[b]) + int(lens[b])].tobytes()
+            assert got == p, b
+            comp.append(got)
+        else:
+            assert lens[b] == len(blk)
+            comp.append(blk)
+        coffs.append(at)
+        at += len(comp[-1])
+    raw_lens = [min(B, len(data) - b * B) for b in range(len(want))]
+    raw, dcrcs, errs = codec.decompress_arrays(b"".join(comp), coffs, [len(c) for c in comp], methods, raw_lens)
+    assert not errs.any()
+    assert raw.tobytes() == data
+    assert list(dcrcs) == list(crcs)
+
+
+def test_uneven_batch(codec):
+    """Blocks of uneven sizes from many files in one call (partial tails, stored blocks)."""
+    import datagen as G
+    rng = random.Random(9)
+    files = [G.by_kind(k % 3, rng.randrange(1, 150000), 18, 40 + k).tobytes() for k in range(12)]
+    files.append(b"")
+    files.append(b"xyz")
+    B = 1 << 17
+    blob, offs, lens = bytearray(), [], []
+    for f in files:
+        for o in range(0, len(f), B):
+            offs.append(len(blob) + o)
+            lens.append(min(B, len(f) - o))
+        blob += f
+        blob += b"\x55" * rng.randrange(0, 7)  # gaps between files
+    data = bytes(blob)
+    methods, clens, crcs, pay, poffs = codec.compress_batch_arrays(data, offs, lens, 17, level=5)
+    for b, (o, l) in enumerate(zip(offs, lens)):
+        blk = data[o:o + l]
+        p = O.Port.compress_block(blk, 32)
+        if len(p) >= l:
+            assert methods[b] == 0
+        else:
+            assert methods[b] == 1 and pay[int(poffs[b]): int(poffs[b]) + int(clens[b])].tobytes() == p
+        assert crcs[b] == O.Port.crc32(blk)
+
+
+def test_damaged_payloads_never_fault(codec, manifest):
+    """Random damage: the GPU decoder refuses or returns bytes; where the oracle accepts, the bytes agree."""
+    ent = [e for e in manifest["blocks"] if e["name"] == "mixed_64k"][0]
+    data = block_input(ent)
+    pay = bytearray(block_payload(ent, 5))
+    rng = random.Random(21)
+    refused = 0
+    for _ in range(200):
+        b = bytearray(pay)
+        for _ in range(rng.randrange(1, 40)):
+            b[rng.randrange(len(b))] = rng.randrange(256)
+        if rng.random() < 0.2:
+            b = b[: rng.randrange(len(b))]
+        raw, crcs, errs = codec.decompress_arrays(bytes(b), [0], [len(b)], [1], [len(data)], raise_on_damage=False)
+        cpu = O.Port.decompress_block(bytes(b), len(data))
+        if errs[0]:
+            refused += 1
+        elif cpu is not None:
+            assert raw.tobytes() == cpu
+    assert refused > 0
+    # the codec still works after the damage
+    raw, _, errs = codec.decompress_arrays(bytes(pay), [0], [len(pay)], [1], [len(data)])
+    assert raw.tobytes() == data
+
+
+def test_reference_api_shapes(codec):
+    """compress / decompress through the zero::Codec-shaped methods."""
+    import zero_cuda as Z
+    import datagen as G
+    data = G.lz_mix(300000, 18, 5).tobytes()
+    outs = codec.compress(data, 18)
+    B = 1 << 18
+    ins = []
+    for b, o in enumerate(outs):
+        blk = data[b * B:(b + 1) * B]
+        ins.append(Z.BlockIn(o.method, len(blk), o.data if o.method else blk))
+    assert codec.decompress(ins) == data
+    assert codec.batch_bytes(18) >= B and codec.batch_bytes_decode(18) >= B
+    assert "GPU" in codec.name()

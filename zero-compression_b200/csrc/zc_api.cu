@@ -1,0 +1,616 @@
+// zc_api.cu -- the C ABI of include/zero_cuda.h: device context, scratch sized per block size, batching
+// of host calls into launches, host <-> device copies.  It replaces the reference's GpuCodec
+// (src/gpu_codec.h) and the Level Zero runtime under it (src/gpu.h, src/ze_min.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/zero_cuda.h"
+#include "zc_internal.cuh"
+#include "zc_kernels.h"
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct HostBuf {  // pinned staging
+  void* p = nullptr;
+  size_t n = 0;
+};
+
+__global__ void k_plain_blocks(uint64_t n, uint32_t B, uint32_t nb, uint64_t* off, uint32_t* len) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const uint64_t o = (uint64_t)b * B;
+  off[b] = o;
+  len[b] = (uint32_t)std::min<uint64_t>(B, n - o);
+}
+
+int depth_for_level(int level) { return level <= 1 ? 8 : level >= 9 ? 256 : 32; }
+
+void build_crc_tables(zc::CrcTables& T) {
+  for (uint32_t i = 0; i < 256; ++i) {
+    uint32_t r = i;
+    for (int k = 0; k < 8; ++k) r = (r >> 1) ^ (0xEDB88320u & (0u - (r & 1u)));
+    T.t[0][i] = r;
+  }
+  for (int k = 1; k < 8; ++k)
+    for (uint32_t i = 0; i < 256; ++i) T.t[k][i] = (T.t[k - 1][i] >> 8) ^ T.t[0][T.t[k - 1][i] & 0xFFu];
+  uint32_t p = 0x00800000u;  // x^8
+  for (int e = 0; e < 64; ++e) { T.pow2[e] = p; p = zc::gf2_mul(p, p); }
+}
+
+// per-stage CUDA-event records of one context
+struct StageRecords {
+  struct Rec { const char* name; cudaEvent_t a, b; };
+  std::vector<cudaEvent_t> pool;
+  std::vector<Rec> pending;
+  const char* open_name = nullptr;
+  cudaEvent_t open_ev = nullptr;
+  std::map<std::string, std::pair<double, uint64_t>> totals;
+  std::vector<std::string> order;
+  cudaEvent_t get() {
+    if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void collect() {
+    for (const Rec& r : pending) {
+      float ms = 0;
+      cudaEventSynchronize(r.b);
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      auto it = totals.find(r.name);
+      if (it == totals.end()) { order.push_back(r.name); it = totals.emplace(r.name, std::make_pair(0.0, (uint64_t)0)).first; }
+      it->second.first += ms;
+      it->second.second += 1;
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    pending.clear();
+  }
+  ~StageRecords() {
+    for (const Rec& r : pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (cudaEvent_t e : pool) cudaEventDestroy(e);
+  }
+};
+
+}  // namespace
+
+void zc::Stages::begin(const char* name, cudaStream_t st) {
+  ++launches;
+  if (!timing || !impl) return;
+  StageRecords* R = static_cast<StageRecords*>(impl);
+  R->open_name = name;
+  R->open_ev = R->get();
+  cudaEventRecord(R->open_ev, st);
+}
+void zc::Stages::end(cudaStream_t st) {
+  if (!timing || !impl) return;
+  StageRecords* R = static_cast<StageRecords*>(impl);
+  cudaEvent_t e = R->get();
+  cudaEventRecord(e, st);
+  R->pending.push_back({R->open_name, R->open_ev, e});
+}
+
+struct zc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err, name;
+  uint32_t block_log = 18;
+  int level = 5;
+  zc::Stages stages;
+  StageRecords records;
+  zc::CrcTables* d_crct = nullptr;
+  // encoder scratch for enc_nb blocks of 2^enc_bl bytes
+  uint32_t enc_nb = 0, enc_bl = 0;
+  DevBuf e_tmp_pos, e_srt_pos, e_rank, e_minfo, e_tmp_h, e_srt_h, e_tk_i, e_tk_m, e_tk_d, e_bcnt, e_lit, e_tok,
+      e_ext, e_sym, e_grp, e_bits, e_lanes, e_freq, e_lanelen, e_sinfo, e_slab;
+  // decoder scratch for dec_nb blocks of 2^dec_bl bytes
+  uint32_t dec_nb = 0, dec_bl = 0;
+  DevBuf d_lit, d_tok, d_sym, d_grp, d_ext, d_meta;
+  // staging for the host-pointer calls
+  DevBuf s_in, s_blk, s_out, s_meta;
+  HostBuf h_meta;
+};
+
+namespace {
+
+int fail(zc_ctx* c, int code, const std::string& msg) {
+  c->err = msg;
+  return code;
+}
+int cuda_fail(zc_ctx* c, cudaError_t e, const char* what) {
+  c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? ZC_E_NOMEM : ZC_E_DEVICE;
+}
+#define ZC_CUDA(call)                                  \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+  } while (0)
+
+cudaError_t grow(DevBuf& b, size_t bytes) {
+  if (bytes <= b.n && b.p) return cudaSuccess;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.n = 0;
+  bytes = std::max<size_t>(bytes, 256);
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e == cudaSuccess) b.n = bytes;
+  return e;
+}
+cudaError_t grow_host(HostBuf& b, size_t bytes) {
+  if (bytes <= b.n && b.p) return cudaSuccess;
+  if (b.p) cudaFreeHost(b.p);
+  b.p = nullptr;
+  b.n = 0;
+  cudaError_t e = cudaMallocHost(&b.p, std::max<size_t>(bytes, 4096));
+  if (e == cudaSuccess) b.n = std::max<size_t>(bytes, 4096);
+  return e;
+}
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.n = 0;
+}
+
+int ensure_enc(zc_ctx* c, uint32_t nb, uint32_t block_log) {
+  if (nb <= c->enc_nb && block_log == c->enc_bl) return ZC_OK;
+  const size_t B = (size_t)1 << block_log, TC = zc::tok_cap((uint32_t)B), EC = zc::ext_cap((uint32_t)B);
+  const size_t N = (size_t)nb * B;
+  ZC_CUDA(grow(c->e_tmp_pos, N * 4));
+  ZC_CUDA(grow(c->e_srt_pos, N * 4));
+  ZC_CUDA(grow(c->e_rank, N * 4));
+  ZC_CUDA(grow(c->e_minfo, N * 4));
+  ZC_CUDA(grow(c->e_tmp_h, N * 2));
+  ZC_CUDA(grow(c->e_srt_h, N * 2));
+  ZC_CUDA(grow(c->e_tk_i, nb * TC * 4));
+  ZC_CUDA(grow(c->e_tk_m, nb * TC * 4));
+  ZC_CUDA(grow(c->e_tk_d, nb * TC * 4));
+  ZC_CUDA(grow(c->e_bcnt, (size_t)nb * 8 * 4));
+  ZC_CUDA(grow(c->e_lit, N));
+  ZC_CUDA(grow(c->e_tok, nb * TC));
+  ZC_CUDA(grow(c->e_ext, nb * EC));
+  ZC_CUDA(grow(c->e_sym, nb * TC));
+  ZC_CUDA(grow(c->e_grp, nb * TC));
+  ZC_CUDA(grow(c->e_bits, (size_t)nb * zc::bits_cap((uint32_t)B)));
+  ZC_CUDA(grow(c->e_lanes, (size_t)nb * zc::lanes_per_block((uint32_t)B)));
+  ZC_CUDA(grow(c->e_freq, (size_t)nb * 5 * 256 * 2));
+  ZC_CUDA(grow(c->e_lanelen, (size_t)nb * 5 * 64 * 4));
+  ZC_CUDA(grow(c->e_sinfo, (size_t)nb * 5 * 4 * 4));
+  ZC_CUDA(grow(c->e_slab, N));
+  c->enc_nb = nb;
+  c->enc_bl = block_log;
+  return ZC_OK;
+}
+
+int ensure_dec(zc_ctx* c, uint32_t nb, uint32_t block_log) {
+  if (nb <= c->dec_nb && block_log == c->dec_bl) return ZC_OK;
+  const size_t B = (size_t)1 << block_log, TC = zc::tok_cap((uint32_t)B), EC = zc::ext_cap((uint32_t)B);
+  ZC_CUDA(grow(c->d_lit, (size_t)nb * B));
+  ZC_CUDA(grow(c->d_tok, (size_t)nb * TC));
+  ZC_CUDA(grow(c->d_sym, (size_t)nb * TC));
+  ZC_CUDA(grow(c->d_grp, (size_t)nb * TC));
+  ZC_CUDA(grow(c->d_ext, (size_t)nb * EC));
+  ZC_CUDA(grow(c->d_meta, (size_t)nb * sizeof(zc::DecMeta)));
+  c->dec_nb = nb;
+  c->dec_bl = block_log;
+  return ZC_OK;
+}
+
+bool bad_block_log(uint32_t bl) { return bl < zc::kMinBlockLog || bl > zc::kMaxBlockLog; }
+
+// blocks per encoder launch: about 256 MiB of input, and the grid's y limit
+uint32_t enc_blocks_per_launch(uint32_t block_log) {
+  return (uint32_t)std::min<size_t>(((size_t)256 << 20) >> block_log, 65535);
+}
+uint32_t dec_blocks_per_launch(uint32_t block_log) {
+  return (uint32_t)std::min<size_t>(((size_t)1 << 30) >> block_log, 1u << 20);
+}
+
+int check_launch(zc_ctx* c, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, what);
+  return ZC_OK;
+}
+
+// the encoder over nb device-resident blocks (offsets / lengths on the device)
+int encode_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_off, const uint32_t* d_len, uint32_t nb,
+                  uint32_t block_log, int level, uint8_t* d_methods, uint32_t* d_lens, uint32_t* d_crcs,
+                  uint8_t* d_out, size_t out_cap, uint64_t* d_out_offs, uint64_t* d_total, int emit_stored,
+                  cudaStream_t st) {
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  if (nb > enc_blocks_per_launch(block_log)) return fail(c, ZC_E_ARG, "too many blocks for one launch");
+  if (int r = ensure_enc(c, nb, block_log)) return r;
+  zc::EncArgs A{};
+  A.in = d_in; A.in_off = d_off; A.in_len = d_len; A.nb = nb;
+  A.B = 1u << block_log; A.block_log = block_log; A.depth = depth_for_level(level); A.cmp_cap = 32;
+  A.tmp_pos = c->e_tmp_pos.as<uint32_t>(); A.srt_pos = c->e_srt_pos.as<uint32_t>();
+  A.rank = c->e_rank.as<uint32_t>(); A.minfo = c->e_minfo.as<uint32_t>();
+  A.tmp_h = c->e_tmp_h.as<uint16_t>(); A.srt_h = c->e_srt_h.as<uint16_t>();
+  A.tk_i = c->e_tk_i.as<uint32_t>(); A.tk_m = c->e_tk_m.as<uint32_t>(); A.tk_d = c->e_tk_d.as<uint32_t>();
+  A.bcnt = c->e_bcnt.as<uint32_t>();
+  A.s_lit = c->e_lit.as<uint8_t>(); A.s_tok = c->e_tok.as<uint8_t>(); A.s_ext = c->e_ext.as<uint8_t>();
+  A.s_sym = c->e_sym.as<uint8_t>(); A.s_grp = c->e_grp.as<uint8_t>(); A.s_bits = c->e_bits.as<uint8_t>();
+  A.lanes = c->e_lanes.as<uint8_t>(); A.freq = c->e_freq.as<uint16_t>(); A.lanelen = c->e_lanelen.as<uint32_t>();
+  A.sinfo = c->e_sinfo.as<uint32_t>(); A.slab = c->e_slab.as<uint8_t>();
+  A.out = d_out; A.out_cap = out_cap; A.out_off = d_out_offs; A.out_len = d_lens; A.out_method = d_methods;
+  A.out_total = d_total; A.emit_stored = emit_stored;
+  zc::CrcArgs C{};
+  C.base = d_in; C.offs = d_off; C.lens = d_len; C.nb = nb; C.crc = d_crcs; C.tables = c->d_crct;
+  if (!d_crcs) C.nb = 0;
+  zc::launch_encode(A, C, st, c->stages);
+  return check_launch(c, "encoder launch");
+}
+
+int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs, const uint32_t* d_comp_lens,
+                  const uint8_t* d_methods, const uint32_t* d_raw_lens, uint32_t nb, uint32_t block_log, uint8_t* d_out,
+                  const uint64_t* d_out_offs, uint32_t* d_crcs, uint32_t* d_err, cudaStream_t st) {
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  if (int r = ensure_dec(c, std::max(nb, 1u), block_log)) return r;
+  ZC_CUDA(cudaMemsetAsync(d_err, 0, (size_t)nb * 4, st));
+  zc::DecArgs A{};
+  A.comp = d_comp; A.comp_off = d_comp_offs; A.comp_len = d_comp_lens; A.method = d_methods; A.raw_len = d_raw_lens;
+  A.nb = nb; A.B = 1u << block_log; A.out = d_out; A.out_off = d_out_offs; A.err = d_err;
+  A.s_lit = c->d_lit.as<uint8_t>(); A.s_tok = c->d_tok.as<uint8_t>(); A.s_sym = c->d_sym.as<uint8_t>();
+  A.s_grp = c->d_grp.as<uint8_t>(); A.s_ext = c->d_ext.as<uint8_t>(); A.meta = c->d_meta.as<zc::DecMeta>();
+  zc::launch_decode(A, st, c->stages);
+  if (d_crcs && nb) {
+    zc::CrcArgs C{};
+    C.base = d_out; C.offs = d_out_offs; C.lens = d_raw_lens; C.nb = nb; C.crc = d_crcs; C.err = d_err;
+    C.tables = c->d_crct;
+    zc::launch_crc(C, st, c->stages, "k_crc_out");
+  }
+  return check_launch(c, "decoder launch");
+}
+
+// host-pointer compress of nb blocks whose bytes lie in host memory [lo, lo + span)
+int compress_host(zc_ctx* c, const uint8_t* host_base, const uint64_t* in_offs, const uint32_t* in_lens, uint32_t nb,
+                  uint64_t plain_n, uint32_t block_log, int level, uint8_t* methods, uint32_t* comp_lens,
+                  uint32_t* crcs, uint8_t* payloads, size_t payload_cap, uint64_t* pay_offs) {
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  const uint32_t B = 1u << block_log;
+  const uint32_t per = enc_blocks_per_launch(block_log);
+  cudaStream_t st = c->stream;
+  uint64_t pay_at = 0;
+  for (uint32_t b0 = 0; b0 < nb; b0 += per) {
+    const uint32_t k = std::min(per, nb - b0);
+    // the bytes of blocks b0 .. b0+k-1 as one host span
+    uint64_t lo, hi;
+    if (in_offs) {
+      lo = UINT64_MAX; hi = 0;
+      for (uint32_t b = b0; b < b0 + k; ++b) {
+        if (in_lens[b] > B) return fail(c, ZC_E_ARG, "a block is longer than the block size");
+        lo = std::min(lo, in_offs[b]);
+        hi = std::max(hi, in_offs[b] + in_lens[b]);
+      }
+      if (lo == UINT64_MAX) lo = hi = 0;
+    } else {
+      lo = (uint64_t)b0 * B;
+      hi = std::min<uint64_t>(plain_n, (uint64_t)(b0 + k) * B);
+    }
+    const uint64_t span = hi - lo;
+    ZC_CUDA(grow(c->s_in, span + 64));
+    ZC_CUDA(grow(c->s_blk, (size_t)k * 12));
+    ZC_CUDA(grow(c->s_out, span + 64));
+    const size_t meta_bytes = (size_t)k * (8 + 4 + 4 + 1) + 16;
+    ZC_CUDA(grow(c->s_meta, meta_bytes));
+    ZC_CUDA(grow_host(c->h_meta, meta_bytes + (size_t)k * 12));
+    uint8_t* d_in = c->s_in.as<uint8_t>();
+    uint64_t* d_off = c->s_blk.as<uint64_t>();
+    uint32_t* d_len = reinterpret_cast<uint32_t*>(d_off + k);
+    ZC_CUDA(cudaMemcpyAsync(d_in, host_base + lo, span, cudaMemcpyHostToDevice, st));
+    ZC_CUDA(cudaMemsetAsync(d_in + span, 0, 64, st));
+    if (in_offs) {
+      uint64_t* ho = static_cast<uint64_t*>(c->h_meta.p);
+      uint32_t* hl = reinterpret_cast<uint32_t*>(ho + k);
+      for (uint32_t b = 0; b < k; ++b) { ho[b] = in_offs[b0 + b] - lo; hl[b] = in_lens[b0 + b]; }
+      ZC_CUDA(cudaMemcpyAsync(d_off, ho, (size_t)k * 12, cudaMemcpyHostToDevice, st));
+    } else {
+      c->stages.begin("k_plain_blocks", st);
+      k_plain_blocks<<<(k + 255) / 256, 256, 0, st>>>(span, B, k, d_off, d_len);
+      c->stages.end(st);
+    }
+    uint8_t* m = c->s_meta.as<uint8_t>();
+    uint64_t* d_poff = reinterpret_cast<uint64_t*>(m);
+    uint64_t* d_total = d_poff + k;
+    uint32_t* d_plen = reinterpret_cast<uint32_t*>(d_total + 1);
+    uint32_t* d_crc = d_plen + k;
+    uint8_t* d_meth = reinterpret_cast<uint8_t*>(d_crc + k);
+    if (int r = encode_device(c, d_in, d_off, d_len, k, block_log, level, d_meth, d_plen, d_crc, c->s_out.as<uint8_t>(),
+                              c->s_out.n, d_poff, d_total, 0, st))
+      return r;
+    ZC_CUDA(cudaMemcpyAsync(c->h_meta.p, m, meta_bytes, cudaMemcpyDeviceToHost, st));
+    ZC_CUDA(cudaStreamSynchronize(st));
+    const uint8_t* hm = static_cast<const uint8_t*>(c->h_meta.p);
+    const uint64_t* h_poff = reinterpret_cast<const uint64_t*>(hm);
+    const uint64_t total = h_poff[k];
+    const uint32_t* h_plen = reinterpret_cast<const uint32_t*>(h_poff + k + 1);
+    const uint32_t* h_crc = h_plen + k;
+    const uint8_t* h_meth = reinterpret_cast<const uint8_t*>(h_crc + k);
+    if (pay_at + total > payload_cap) return fail(c, ZC_E_ARG, "payload buffer too small");
+    if (total) ZC_CUDA(cudaMemcpyAsync(payloads + pay_at, c->s_out.p, total, cudaMemcpyDeviceToHost, st));
+    for (uint32_t b = 0; b < k; ++b) {
+      methods[b0 + b] = h_meth[b];
+      comp_lens[b0 + b] = h_plen[b];
+      if (crcs) crcs[b0 + b] = h_crc[b];
+      if (pay_offs) pay_offs[b0 + b] = h_meth[b] ? pay_at + h_poff[b] : 0;
+    }
+    ZC_CUDA(cudaStreamSynchronize(st));
+    pay_at += total;
+  }
+  return ZC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zc_open(zc_ctx** out, int device) {
+  if (!out) return ZC_E_ARG;
+  *out = nullptr;
+  zc_ctx* c = new zc_ctx;
+  c->device = device;
+  c->stages.impl = &c->records;
+  cudaError_t e = cudaSetDevice(device);
+  cudaDeviceProp prop;
+  if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, device);
+  if (e == cudaSuccess && prop.major < 10) {
+    c->err = "the sm_100a kernels need a Blackwell (compute 10.x) GPU";
+    *out = c;
+    return ZC_E_DEVICE;
+  }
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_crct, sizeof(zc::CrcTables));
+  if (e == cudaSuccess) {
+    zc::CrcTables T;
+    build_crc_tables(T);
+    e = cudaMemcpy(c->d_crct, &T, sizeof T, cudaMemcpyHostToDevice);
+  }
+  *out = c;
+  if (e != cudaSuccess) return cuda_fail(c, e, "opening the GPU");
+  char b[512];
+  snprintf(b, sizeof b, "GPU %s (CUDA, %d SMs)", prop.name, prop.multiProcessorCount);
+  c->name = b;
+  return ZC_OK;
+}
+
+void zc_close(zc_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_rank, &c->e_minfo, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
+                    &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
+                    &c->e_bits, &c->e_lanes, &c->e_freq, &c->e_lanelen, &c->e_sinfo, &c->e_slab, &c->d_lit, &c->d_tok,
+                    &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta})
+    release(*b);
+  if (c->h_meta.p) cudaFreeHost(c->h_meta.p);
+  if (c->d_crct) cudaFree(c->d_crct);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* zc_last_error(const zc_ctx* c) { return c ? c->err.c_str() : "no context"; }
+const char* zc_name(const zc_ctx* c) { return c ? c->name.c_str() : ""; }
+uint64_t zc_launch_count(const zc_ctx* c) { return c ? c->stages.launches : 0; }
+
+int zc_profile(zc_ctx* c, int on) {
+  if (!c) return ZC_E_ARG;
+  ZC_CUDA(cudaSetDevice(c->device));
+  c->records.collect();
+  c->records.totals.clear();
+  c->records.order.clear();
+  c->stages.timing = on != 0;
+  return ZC_OK;
+}
+
+int zc_profile_stages(zc_ctx* c, uint32_t max, char* names, double* ms, uint64_t* counts, uint32_t* n_out) {
+  if (!c || !n_out) return ZC_E_ARG;
+  ZC_CUDA(cudaSetDevice(c->device));
+  c->records.collect();
+  const uint32_t n = (uint32_t)c->records.order.size();
+  *n_out = n;
+  for (uint32_t i = 0; i < n && i < max; ++i) {
+    const std::string& k = c->records.order[i];
+    const auto& v = c->records.totals[k];
+    if (names) { strncpy(names + 32 * i, k.c_str(), 31); names[32 * i + 31] = 0; }
+    if (ms) ms[i] = v.first;
+    if (counts) counts[i] = v.second;
+  }
+  return ZC_OK;
+}
+
+int zc_prepare(zc_ctx* c, uint32_t block_log, int level) {
+  if (!c) return ZC_E_ARG;
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  c->block_log = block_log;
+  c->level = level;
+  return ZC_OK;
+}
+
+size_t zc_batch_bytes(const zc_ctx*, uint32_t block_log) { return (size_t)enc_blocks_per_launch(block_log) << block_log; }
+size_t zc_batch_bytes_decode(const zc_ctx*, uint32_t block_log) {
+  return (size_t)dec_blocks_per_launch(block_log) << block_log;
+}
+
+int zc_compress(zc_ctx* c, const uint8_t* in, size_t n, uint32_t block_log, int level, uint8_t* methods,
+                uint32_t* comp_lens, uint32_t* crcs, uint8_t* payloads, size_t payload_cap, uint64_t* pay_offs) {
+  if (!c) return ZC_E_ARG;
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  ZC_CUDA(cudaSetDevice(c->device));
+  const uint64_t B = 1ull << block_log;
+  const uint64_t nb = (n + B - 1) / B;
+  if (nb > 0xFFFFFFFFull) return fail(c, ZC_E_ARG, "too many blocks");
+  return compress_host(c, in, nullptr, nullptr, (uint32_t)nb, n, block_log, level, methods, comp_lens, crcs, payloads,
+                       payload_cap, pay_offs);
+}
+
+int zc_compress_batch(zc_ctx* c, const uint8_t* in, const uint64_t* in_offs, const uint32_t* in_lens, uint32_t nb,
+                      uint32_t block_log, int level, uint8_t* methods, uint32_t* comp_lens, uint32_t* crcs,
+                      uint8_t* payloads, size_t payload_cap, uint64_t* pay_offs) {
+  if (!c) return ZC_E_ARG;
+  if (nb && (!in_offs || !in_lens)) return fail(c, ZC_E_ARG, "block offsets and lengths are required");
+  ZC_CUDA(cudaSetDevice(c->device));
+  return compress_host(c, in, in_offs, in_lens, nb, 0, block_log, level, methods, comp_lens, crcs, payloads,
+                       payload_cap, pay_offs);
+}
+
+int zc_compress_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_in_offs, const uint32_t* d_in_lens,
+                       uint32_t nb, uint32_t block_log, int level, uint8_t* d_methods, uint32_t* d_comp_lens,
+                       uint32_t* d_crcs, uint8_t* d_out, size_t out_cap, uint64_t* d_out_offs, uint64_t* d_total,
+                       void* stream) {
+  if (!c) return ZC_E_ARG;
+  ZC_CUDA(cudaSetDevice(c->device));
+  return encode_device(c, d_in, d_in_offs, d_in_lens, nb, block_log, level, d_methods, d_comp_lens, d_crcs, d_out,
+                       out_cap, d_out_offs, d_total, 1, static_cast<cudaStream_t>(stream));
+}
+
+int zc_decompress_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs, const uint32_t* d_comp_lens,
+                         const uint8_t* d_methods, const uint32_t* d_raw_lens, uint32_t nb, uint32_t block_log,
+                         uint8_t* d_out, const uint64_t* d_out_offs, uint32_t* d_crcs, uint32_t* d_err, void* stream) {
+  if (!c) return ZC_E_ARG;
+  ZC_CUDA(cudaSetDevice(c->device));
+  if (nb > dec_blocks_per_launch(block_log)) return fail(c, ZC_E_ARG, "too many blocks for one launch");
+  return decode_device(c, d_comp, d_comp_offs, d_comp_lens, d_methods, d_raw_lens, nb, block_log, d_out, d_out_offs,
+                       d_crcs, d_err, static_cast<cudaStream_t>(stream));
+}
+
+int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, const uint32_t* comp_lens,
+                  const uint8_t* methods, const uint32_t* raw_lens, uint32_t nb, uint8_t* out, uint32_t* crcs_out,
+                  uint32_t* block_err) {
+  if (!c) return ZC_E_ARG;
+  ZC_CUDA(cudaSetDevice(c->device));
+  uint32_t maxraw = 0;
+  for (uint32_t b = 0; b < nb; ++b) maxraw = std::max(maxraw, raw_lens[b]);
+  uint32_t bl = zc::kMinBlockLog;
+  while (bl < zc::kMaxBlockLog && (1u << bl) < maxraw) ++bl;
+  if (maxraw > (1u << zc::kMaxBlockLog)) return fail(c, ZC_E_DATA, "a block is longer than 1 MiB");
+  const uint32_t per = dec_blocks_per_launch(bl);
+  cudaStream_t st = c->stream;
+  uint64_t out_at = 0;
+  int status = ZC_OK;
+  for (uint32_t b0 = 0; b0 < nb; b0 += per) {
+    const uint32_t k = std::min(per, nb - b0);
+    uint64_t lo = UINT64_MAX, hi = 0, raw_total = 0, comp_sum = 0;
+    for (uint32_t b = b0; b < b0 + k; ++b) {
+      lo = std::min(lo, comp_offs[b]);
+      hi = std::max(hi, comp_offs[b] + comp_lens[b]);
+      raw_total += raw_lens[b];
+      comp_sum += comp_lens[b];
+    }
+    if (lo == UINT64_MAX) lo = hi = 0;
+    // one copy of the span when the blocks lie close together (an archive's records), else gathered
+    const bool gather = hi - lo > comp_sum + comp_sum / 2 + 4096;
+    const uint64_t span = gather ? comp_sum : hi - lo;
+    ZC_CUDA(grow(c->s_in, span + 64));
+    ZC_CUDA(grow(c->s_out, raw_total + 64));
+    const size_t per_blk = 8 + 8 + 4 + 4 + 4 + 4 + 1;
+    ZC_CUDA(grow(c->s_blk, (size_t)k * per_blk + 64));
+    ZC_CUDA(grow_host(c->h_meta, (size_t)k * per_blk + 64 + (gather ? 0 : 0)));
+    uint8_t* hb = static_cast<uint8_t*>(c->h_meta.p);
+    uint64_t* h_coff = reinterpret_cast<uint64_t*>(hb);
+    uint64_t* h_ooff = h_coff + k;
+    uint32_t* h_clen = reinterpret_cast<uint32_t*>(h_ooff + k);
+    uint32_t* h_rlen = h_clen + k;
+    uint32_t* h_crc = h_rlen + k;
+    uint32_t* h_err = h_crc + k;
+    uint8_t* h_meth = reinterpret_cast<uint8_t*>(h_err + k);
+    uint64_t g = 0, o = 0;
+    for (uint32_t b = 0; b < k; ++b) {
+      const uint32_t j = b0 + b;
+      h_coff[b] = gather ? g : comp_offs[j] - lo;
+      g += comp_lens[j];
+      h_ooff[b] = o;
+      o += raw_lens[j];
+      h_clen[b] = comp_lens[j];
+      h_rlen[b] = raw_lens[j];
+      h_meth[b] = methods[j];
+    }
+    uint8_t* d_in = c->s_in.as<uint8_t>();
+    if (gather) {
+      for (uint32_t b = 0; b < k; ++b)
+        if (comp_lens[b0 + b])
+          ZC_CUDA(cudaMemcpyAsync(d_in + h_coff[b], comp + comp_offs[b0 + b], comp_lens[b0 + b], cudaMemcpyHostToDevice, st));
+    } else if (span) {
+      ZC_CUDA(cudaMemcpyAsync(d_in, comp + lo, span, cudaMemcpyHostToDevice, st));
+    }
+    uint8_t* db = c->s_blk.as<uint8_t>();
+    ZC_CUDA(cudaMemcpyAsync(db, hb, (size_t)k * per_blk, cudaMemcpyHostToDevice, st));
+    uint64_t* d_coff = reinterpret_cast<uint64_t*>(db);
+    uint64_t* d_ooff = d_coff + k;
+    uint32_t* d_clen = reinterpret_cast<uint32_t*>(d_ooff + k);
+    uint32_t* d_rlen = d_clen + k;
+    uint32_t* d_crc = d_rlen + k;
+    uint32_t* d_err = d_crc + k;
+    uint8_t* d_meth = reinterpret_cast<uint8_t*>(d_err + k);
+    if (int r = decode_device(c, d_in, d_coff, d_clen, d_meth, d_rlen, k, bl, c->s_out.as<uint8_t>(), d_ooff, d_crc,
+                              d_err, st))
+      return r;
+    if (raw_total) ZC_CUDA(cudaMemcpyAsync(out + out_at, c->s_out.p, raw_total, cudaMemcpyDeviceToHost, st));
+    ZC_CUDA(cudaMemcpyAsync(h_crc, d_crc, (size_t)k * 8, cudaMemcpyDeviceToHost, st));
+    ZC_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t b = 0; b < k; ++b) {
+      if (crcs_out) crcs_out[b0 + b] = h_crc[b];
+      if (block_err) block_err[b0 + b] = h_err[b];
+      if (h_err[b] && status == ZC_OK) {
+        status = ZC_E_DATA;
+        char m[128];
+        snprintf(m, sizeof m, "block %u damaged (GPU decoder, code %u)", b0 + b, h_err[b]);
+        c->err = m;
+      }
+    }
+    out_at += raw_total;
+  }
+  return status;
+}
+
+int zc_crc32(zc_ctx* c, const uint8_t* data, size_t n, uint32_t* crc) {
+  if (!c || !crc) return ZC_E_ARG;
+  ZC_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = c->stream;
+  const size_t piece = (size_t)1 << 20;
+  const uint32_t nb = (uint32_t)((n + piece - 1) / piece);
+  ZC_CUDA(grow(c->s_in, n + 64));
+  ZC_CUDA(grow(c->s_blk, (size_t)nb * 16 + 64));
+  ZC_CUDA(grow_host(c->h_meta, (size_t)nb * 16 + 64));
+  if (n) ZC_CUDA(cudaMemcpyAsync(c->s_in.p, data, n, cudaMemcpyHostToDevice, st));
+  uint64_t* d_off = c->s_blk.as<uint64_t>();
+  uint32_t* d_len = reinterpret_cast<uint32_t*>(d_off + nb);
+  uint32_t* d_crc = d_len + nb;
+  c->stages.begin("k_plain_blocks", st);
+  k_plain_blocks<<<(nb + 255) / 256 + 1, 256, 0, st>>>(n, (uint32_t)piece, nb, d_off, d_len);
+  c->stages.end(st);
+  zc::CrcArgs C{};
+  C.base = c->s_in.as<uint8_t>(); C.offs = d_off; C.lens = d_len; C.nb = nb; C.crc = d_crc; C.tables = c->d_crct;
+  zc::launch_crc(C, st, c->stages, "k_crc_in");
+  if (int r = check_launch(c, "crc launch")) return r;
+  uint32_t* h = static_cast<uint32_t*>(c->h_meta.p);
+  ZC_CUDA(cudaMemcpyAsync(h, d_crc, (size_t)nb * 4, cudaMemcpyDeviceToHost, st));
+  ZC_CUDA(cudaStreamSynchronize(st));
+  uint32_t r = 0;
+  for (uint32_t b = 0; b < nb; ++b) r = zc_crc32_combine(r, h[b], std::min<uint64_t>(piece, n - (uint64_t)b * piece));
+  *crc = r;
+  return ZC_OK;
+}
+
+uint32_t zc_crc32_combine(uint32_t a, uint32_t b, uint64_t len_b) {
+  if (!len_b) return a;
+  uint32_t x = 0x80000000u, base = 0x00800000u;  // x^0, x^8
+  for (uint64_t n = len_b; n; n >>= 1) {
+    if (n & 1u) x = zc::gf2_mul(x, base);
+    base = zc::gf2_mul(base, base);
+  }
+  return zc::gf2_mul(x, a) ^ b;
+}
+
+}  // extern "C"

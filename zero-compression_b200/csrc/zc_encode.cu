@@ -1,0 +1,671 @@
+// zc_encode.cu -- the ZB2 block encoder on sm_100a.  It writes, at each level, exactly the payload the
+// reference CPU codec writes (src/codec2.h:43-153 with the depth of src/main.cpp:45, 54).
+//
+// The CPU parse walks hash chains: for position i, the `depth` most recent earlier positions whose
+// 4-byte hash (16 bits) equals i's, the longest match kept (the nearest on a tie), one lazy step.  A
+// chain is exactly the run of i's predecessors in a stable sort of the positions by hash, so:
+//
+//   k_enc_sort     one CTA per block: stable two-pass LSD radix sort of the positions by hash
+//                  (8 + 8 bits; per-warp histograms, warp match_any ranks; no global atomics)
+//   k_enc_match    one thread per sorted position: scans its chain, comparing at most cmp_cap bytes;
+//                  a match that reaches cmp_cap is marked and finished only if the parse visits it
+//   k_enc_parse    one CTA per block: the greedy + lazy parse as a chain 0 -> next(0) -> ..., walked
+//                  per segment in parallel from the segment start, then re-walked from the true entry
+//                  until it meets the first walk (rounds until no segment exit moves)
+//   k_enc_streams  one warp per block: groups, recent offsets, tok / ext / sym / group streams, offset
+//                  bits (a warp-private bit window, no atomics on global memory), literals
+//   k_enc_rans     one CTA per (block, stream): histogram, 12-bit normalisation with the reference's
+//                  tie-breaks, 64 lanes coding backwards (src/codec.h:41-147)
+//   k_enc_pack     one CTA per block: the payload (src/codec2.h:139-152), or "stored"
+//   k_enc_scan / k_enc_emit: record sizes -> offsets, payloads packed back to back
+#include "zc_internal.cuh"
+#include "zc_kernels.h"
+
+namespace zc {
+
+// per-position match record: NONE, SAT (longest candidate reached cmp_cap: finish on demand), or the
+// exact (length - 4) << 20 | (distance - 1); lengths are <= 4096, so the top 12 bits never read 0xFFF
+constexpr uint32_t M_NONE = 0xFFFFFFFFu;
+constexpr uint32_t M_SAT = 0xFFF00000u;
+__device__ __forceinline__ uint32_t m_pack(uint32_t m, uint32_t d) { return ((m - 4u) << 20) | (d - 1u); }
+__device__ __forceinline__ uint32_t m_len(uint32_t v) { return (v >> 20) + 4u; }
+__device__ __forceinline__ uint32_t m_dist(uint32_t v) { return (v & 0xFFFFFu) + 1u; }
+
+// 4 bytes at byte offset x of a 4-aligned buffer, from the two aligned words around it
+__device__ __forceinline__ uint32_t load4(const uint8_t* base, uint64_t x) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(base) + (x >> 2);
+  return __funnelshift_r(__ldg(w), __ldg(w + 1), (uint32_t)(x & 3u) * 8u);
+}
+// the CPU parse's hash: 4 bytes times 2654435761, top 16 bits (src/codec2.h:47)
+__device__ __forceinline__ uint32_t hash16(const uint8_t* base, uint64_t x) { return (load4(base, x) * 2654435761u) >> 16; }
+
+// common prefix of the bytes at a and b, at most cap
+__device__ __forceinline__ uint32_t lcp(const uint8_t* base, uint64_t a, uint64_t b, uint32_t cap) {
+  uint32_t l = 0;
+  while (l + 4 <= cap) {
+    const uint32_t x = load4(base, a + l) ^ load4(base, b + l);
+    if (x) return l + ((uint32_t)__ffs(x) - 1u) / 8u;
+    l += 4;
+  }
+  if (l < cap) {
+    const uint32_t x = load4(base, a + l) ^ load4(base, b + l);
+    const uint32_t k = x ? ((uint32_t)__ffs(x) - 1u) / 8u : 4u;
+    return l + min(k, cap - l);
+  }
+  return l;
+}
+
+// ---------------------------------------------------------------- 1. stable sort by hash
+__global__ void __launch_bounds__(1024) k_enc_sort(EncArgs A) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t n = A.in_len[b];
+  const uint32_t count = n >= 4 ? n - 3 : 0;  // positions with 4 bytes left (src/codec2.h:52, 58)
+  if (!count) return;
+  __shared__ uint32_t hist[32][256];
+  __shared__ uint32_t tot[256];
+  const uint32_t tid = threadIdx.x, w = tid >> 5, lane = tid & 31u;
+  const uint32_t cw = (count + 31) / 32;
+  const uint32_t beg = min(w * cw, count), end = min(beg + cw, count);
+  const uint64_t base = A.in_off[b];
+  const size_t so = (size_t)b * A.B;
+  uint32_t* tpos = A.tmp_pos + so;
+  uint16_t* th = A.tmp_h + so;
+  uint32_t* spos = A.srt_pos + so;
+  uint16_t* sh = A.srt_h + so;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (uint32_t i = tid; i < 32 * 256; i += blockDim.x) (&hist[0][0])[i] = 0;
+    __syncthreads();
+    for (uint32_t i = beg + lane; i < end; i += 32) {
+      const uint32_t h = pass == 0 ? hash16(A.in, base + i) : th[i];
+      atomicAdd(&hist[w][pass == 0 ? (h & 0xFFu) : (h >> 8)], 1u);
+    }
+    __syncthreads();
+    if (tid < 256) {
+      uint32_t run = 0;
+      for (uint32_t k = 0; k < 32; ++k) { const uint32_t c = hist[k][tid]; hist[k][tid] = run; run += c; }
+      tot[tid] = run;
+    }
+    __syncthreads();
+    if (w == 0) {
+      uint32_t v[8], s = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { v[k] = tot[lane * 8 + k]; s += v[k]; }
+      uint32_t ex = warp_incl_scan(s) - s;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { tot[lane * 8 + k] = ex; ex += v[k]; }
+    }
+    __syncthreads();
+    if (tid < 256)
+      for (uint32_t k = 0; k < 32; ++k) hist[k][tid] += tot[tid];
+    __syncthreads();
+    for (uint32_t i0 = beg; i0 < end; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      const bool on = i < end;
+      uint32_t h = 0, p = 0;
+      if (on) {
+        if (pass == 0) { p = i; h = hash16(A.in, base + i); }
+        else { p = tpos[i]; h = th[i]; }
+      }
+      const uint32_t d = pass == 0 ? (h & 0xFFu) : (h >> 8);
+      const unsigned act = __ballot_sync(kFull, on);
+      if (on) {
+        const unsigned peers = __match_any_sync(act, d);
+        const uint32_t rk = __popc(peers & ((1u << lane) - 1u));
+        const uint32_t dest = hist[w][d] + rk;
+        if (pass == 0) { tpos[dest] = p; th[dest] = (uint16_t)h; }
+        else { spos[dest] = p; sh[dest] = (uint16_t)h; }
+        __syncwarp(act);
+        if (rk == 0) hist[w][d] += __popc(peers);
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- 2. capped matches at every position
+__global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
+  const uint32_t b = blockIdx.y;
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t n = A.in_len[b];
+  const uint32_t count = n >= 4 ? n - 3 : 0;
+  const size_t so = (size_t)b * A.B;
+  if (r >= count) { if (r < n) A.minfo[so + r] = M_NONE; return; }
+  const uint32_t* spos = A.srt_pos + so;
+  const uint16_t* sh = A.srt_h + so;
+  const uint32_t p = spos[r], h = sh[r];
+  A.rank[so + p] = r;
+  const uint64_t base = A.in_off[b];
+  const uint32_t lim = min(kMaxMatch, n - p), cap = min(A.cmp_cap, lim);
+  const uint64_t ap = base + p;
+  uint32_t best = 0, bd = 0;
+  const uint32_t kmax = min((uint32_t)A.depth, r);
+  for (uint32_t k = 1; k <= kmax; ++k) {
+    if (sh[r - k] != h) break;
+    const uint32_t j = spos[r - k];
+    const uint64_t aj = base + j;
+    if (best && __ldg(A.in + aj + best) != __ldg(A.in + ap + best)) continue;
+    const uint32_t l = lcp(A.in, aj, ap, cap);
+    if (l > best) {
+      best = l;
+      bd = p - j;
+      if (best == cap) break;
+    }
+  }
+  uint32_t v;
+  if (best < 4) v = M_NONE;
+  else if (best == cap && cap < lim) v = M_SAT;
+  else v = m_pack(best, bd);
+  A.minfo[so + p] = v;
+}
+
+// ---------------------------------------------------------------- 3. the parse
+struct ParseBlock {
+  const uint8_t* in;
+  uint64_t base;
+  uint32_t n, depth;
+  uint32_t* minfo;
+  const uint32_t* rank;
+  const uint32_t* spos;
+  const uint16_t* sh;
+};
+
+// the exact match at p (finishing a capped one: the whole chain compared up to 4096 bytes)
+__device__ uint32_t exact_match(const ParseBlock& P, uint32_t p) {
+  const uint32_t v = P.minfo[p];
+  if (v != M_SAT) return v;
+  const uint32_t r = P.rank[p], h = P.sh[r];
+  const uint32_t lim = min(kMaxMatch, P.n - p);
+  const uint64_t ap = P.base + p;
+  uint32_t best = 0, bd = 0;
+  const uint32_t kmax = min(P.depth, r);
+  for (uint32_t k = 1; k <= kmax; ++k) {
+    if (P.sh[r - k] != h) break;
+    const uint32_t j = P.spos[r - k];
+    const uint64_t aj = P.base + j;
+    const uint32_t probe = min(best, lim - 1);
+    if (best && __ldg(P.in + aj + probe) != __ldg(P.in + ap + probe)) continue;
+    const uint32_t l = lcp(P.in, aj, ap, lim);
+    if (l > best) {
+      best = l;
+      bd = p - j;
+      if (best == lim) break;
+    }
+  }
+  const uint32_t e = m_pack(best, bd);
+  P.minfo[p] = e;  // (every thread that finishes it writes the same value)
+  return e;
+}
+
+// one step of the CPU parse from position p (src/codec2.h:69-80): returns the next position; a token,
+// when the step emits one, in (ti, tm, td)
+__device__ __forceinline__ uint32_t parse_step(const ParseBlock& P, uint32_t p, bool& tok, uint32_t& ti, uint32_t& tm,
+                                               uint32_t& td) {
+  const uint32_t v = exact_match(P, p);
+  if (v == M_NONE) { tok = false; return p + 1; }
+  uint32_t m = m_len(v), d = m_dist(v), at = p;
+  if (p + 1 < P.n && P.minfo[p + 1] != M_NONE) {
+    const uint32_t v2 = exact_match(P, p + 1);
+    const uint32_t m2 = m_len(v2), d2 = m_dist(v2);
+    if ((int)(8 * m2) - (int)bitlen(d2) - 8 > (int)(8 * m) - (int)bitlen(d)) { at = p + 1; m = m2; d = d2; }
+  }
+  tok = true; ti = at; tm = m; td = d;
+  return at + m;
+}
+__device__ __forceinline__ uint32_t parse_next(const ParseBlock& P, uint32_t p) {
+  bool t; uint32_t a, c, d;
+  return parse_step(P, p, t, a, c, d);
+}
+
+__global__ void __launch_bounds__(256) k_enc_parse(EncArgs A) {
+  const uint32_t b = blockIdx.x, q = threadIdx.x;
+  const uint32_t n = A.in_len[b];
+  const size_t so = (size_t)b * A.B;
+  __shared__ uint32_t ent[256], ex[256], wsum[8];
+  ParseBlock P;
+  P.in = A.in; P.base = A.in_off[b]; P.n = n; P.depth = (uint32_t)A.depth;
+  P.minfo = A.minfo + so; P.rank = A.rank + so; P.spos = A.srt_pos + so; P.sh = A.srt_h + so;
+  const uint32_t S = max(1u, (n + 255) / 256);
+  const uint32_t s = min(q * S, n), e = min(s + S, n);
+  // round 0: every segment walked from its own start
+  {
+    uint32_t p = s;
+    while (p < e) p = parse_next(P, p);
+    ent[q] = s;
+    ex[q] = s < e ? p : s;
+  }
+  // rounds: each segment re-walked from where the chain before it leaves, until it meets its old walk
+  for (;;) {
+    __syncthreads();
+    const uint32_t want = q == 0 ? 0u : ex[q - 1];
+    __syncthreads();
+    bool changed = false;
+    const uint32_t old_ent = ent[q], old_ex = ex[q];
+    if (want != old_ent) {
+      uint32_t nx;
+      if (want >= e) {
+        nx = want;
+      } else if (old_ent >= e) {
+        uint32_t a = want;
+        while (a < e) a = parse_next(P, a);
+        nx = a;
+      } else {
+        uint32_t a = want, c = old_ent;
+        for (;;) {
+          if (a == c) { nx = old_ex; break; }
+          if (a >= e && c >= e) { nx = a; break; }
+          if (a < c) a = parse_next(P, a); else c = parse_next(P, c);
+        }
+      }
+      ent[q] = want;
+      if (nx != old_ex) { ex[q] = nx; changed = true; }
+    }
+    if (!__syncthreads_or(changed)) break;
+  }
+  // tokens: count per segment, offsets, then write
+  const uint32_t from = ent[q];
+  uint32_t cnt = 0;
+  for (uint32_t p = from; p < e;) {
+    bool t; uint32_t a, c, d;
+    p = parse_step(P, p, t, a, c, d);
+    cnt += t;
+  }
+  const uint32_t incl = warp_incl_scan(cnt);
+  if (lane_id() == 31) wsum[q >> 5] = incl;
+  __syncthreads();
+  uint32_t off = incl - cnt;
+  for (uint32_t k = 0; k < (q >> 5); ++k) off += wsum[k];
+  const size_t to = (size_t)b * tok_cap(A.B);
+  for (uint32_t p = from; p < e;) {
+    bool t; uint32_t a, c, d;
+    p = parse_step(P, p, t, a, c, d);
+    if (t) { A.tk_i[to + off] = a; A.tk_m[to + off] = c; A.tk_d[to + off] = d; ++off; }
+  }
+  if (q == 255) A.bcnt[b * 8 + 0] = off;
+}
+
+// ---------------------------------------------------------------- 4. tokens -> streams
+__global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
+  const uint32_t w = threadIdx.x >> 5, lane = lane_id();
+  const uint32_t b = blockIdx.x * 4 + w;
+  __shared__ uint32_t win[4][24];
+  if (b >= A.nb) return;
+  const uint32_t n = A.in_len[b], nt = A.bcnt[b * 8 + 0];
+  const uint8_t* src = A.in + A.in_off[b];
+  const size_t TC = tok_cap(A.B);
+  const uint32_t* TI = A.tk_i + (size_t)b * TC;
+  const uint32_t* TM = A.tk_m + (size_t)b * TC;
+  const uint32_t* TD = A.tk_d + (size_t)b * TC;
+  uint8_t* lit = A.s_lit + (size_t)b * A.B;
+  uint8_t* tok = A.s_tok + (size_t)b * TC;
+  uint8_t* sym = A.s_sym + (size_t)b * TC;
+  uint8_t* grp = A.s_grp + (size_t)b * TC;
+  uint8_t* ext = A.s_ext + (size_t)b * ext_cap(A.B);
+  uint32_t* bitw = reinterpret_cast<uint32_t*>(A.s_bits + (size_t)b * bits_cap(A.B));
+  if (lane < 24) win[w][lane] = 0;
+  __syncwarp();
+  uint32_t op = 0, gstart = 0, gt = 0, ng = 0, ei = 0, li = 0;
+  uint64_t bp = 0, wbase = 0;
+  uint32_t r0 = 1, r1 = 4, r2 = 8, l0 = 1, l1 = 4, l2 = 8;
+  for (uint32_t t0 = 0; t0 < nt; t0 += 32) {
+    const uint32_t c = min(32u, nt - t0);
+    const uint32_t q = t0 + lane;
+    const bool on = lane < c;
+    const uint32_t i = on ? TI[q] : 0u, m = on ? TM[q] : 4u, d = on ? TD[q] : 1u;
+    const uint32_t endk = i + m;
+    const uint32_t prev_end = __shfl_up_sync(kFull, endk, 1);
+    const uint32_t opk = lane == 0 ? op : prev_end;
+    const uint32_t L = on ? i - opk : 0u;
+    const uint32_t j = i - d, reach = j + min(m, d);
+    // groups (src/codec2.h:103-116): close at 255 tokens, or before a match that reads its own group
+    uint32_t sv = 0, lo = 0;
+    while (lo < c) {
+      const bool viol = on && lane >= lo &&
+                        ((j < opk && reach > gstart && !(lane == lo && gt == 0)) || gt + (lane - lo) >= kMaxGroup);
+      const unsigned vb = __ballot_sync(kFull, viol);
+      const uint32_t first = vb ? (uint32_t)__ffs(vb) - 1u : c;
+      if (lane >= lo && lane < first) sv = d == r0 ? kSymRep : d == r1 ? kSymRep + 1 : d == r2 ? kSymRep + 2 : bitlen(d);
+      for (uint32_t k = first > lo + 3 ? first - 3 : lo; k < first; ++k) {
+        const uint32_t v = __shfl_sync(kFull, d, k);
+        l2 = l1; l1 = l0; l0 = v;
+      }
+      gt += first - lo;
+      if (first < c) {
+        if (gt) { if (lane == 0) grp[ng] = (uint8_t)gt; ++ng; }
+        gt = 0;
+        gstart = __shfl_sync(kFull, opk, first);
+        r0 = l0; r1 = l1; r2 = l2;
+      }
+      lo = first;
+    }
+    if (on) {
+      tok[q] = (uint8_t)((min(L, 15u) << 4) | min(m - 4u, 15u));
+      sym[q] = (uint8_t)sv;
+    }
+    const uint32_t fl = on && L >= 15u, fm = on && m >= 19u;
+    const uint32_t nx = 3u * fl + 2u * fm;
+    const uint32_t xincl = warp_incl_scan(nx);
+    const uint32_t xq = ei + xincl - nx;
+    if (fl) { const uint32_t v = L - 15u; ext[xq] = (uint8_t)v; ext[xq + 1] = (uint8_t)(v >> 8); ext[xq + 2] = (uint8_t)(v >> 16); }
+    if (fm) { const uint32_t v = m - 19u, y = xq + 3u * fl; ext[y] = (uint8_t)v; ext[y + 1] = (uint8_t)(v >> 8); }
+    // offset bits, LSB first, through the warp's window of 24 words
+    const uint32_t nbit = (on && sv < kSymRep) ? sv : 0u;
+    const uint32_t bincl = warp_incl_scan(nbit);
+    if (nbit) {
+      const uint32_t val = d - (1u << nbit);
+      const uint32_t rel = (uint32_t)(bp + bincl - nbit - wbase);
+      const uint32_t sh = rel & 31u;
+      atomicOr(&win[w][rel >> 5], val << sh);
+      if (sh + nbit > 32u) atomicOr(&win[w][(rel >> 5) + 1], val >> (32u - sh));
+    }
+    __syncwarp();
+    bp += __shfl_sync(kFull, bincl, 31);
+    const uint32_t full = (uint32_t)((bp - wbase) >> 5);
+    if (lane < full) bitw[(wbase >> 5) + lane] = win[w][lane];
+    const uint32_t carry = win[w][full];
+    __syncwarp();
+    if (lane < 24) win[w][lane] = lane == 0 ? carry : 0u;
+    __syncwarp();
+    wbase += 32ull * full;
+    // literals before each token
+    const uint32_t lincl = warp_incl_scan(L);
+    const uint32_t lik = li + lincl - L;
+    for (uint32_t k = 0; k < L; ++k) lit[lik + k] = src[opk + k];
+    li += __shfl_sync(kFull, lincl, 31);
+    ei += __shfl_sync(kFull, xincl, 31);
+    op = __shfl_sync(kFull, endk, c - 1);
+  }
+  if (gt && lane == 0) grp[ng] = (uint8_t)gt;
+  if (gt) ++ng;
+  for (uint32_t k = op + lane; k < n; k += 32) lit[li + (k - op)] = src[k];
+  li += n - op;
+  if (bp > wbase && lane == 0) bitw[wbase >> 5] = win[w][0];
+  if (lane == 0) {
+    A.bcnt[b * 8 + 1] = li;
+    A.bcnt[b * 8 + 2] = ei;
+    A.bcnt[b * 8 + 3] = (uint32_t)((bp + 7) / 8);
+    A.bcnt[b * 8 + 4] = ng;
+  }
+}
+
+// ---------------------------------------------------------------- 5. rANS, per (block, stream)
+__device__ __forceinline__ const uint8_t* stream_syms(const EncArgs& A, uint32_t b, uint32_t s) {
+  const size_t TC = tok_cap(A.B);
+  switch (s) {
+    case 0: return A.s_lit + (size_t)b * A.B;
+    case 1: return A.s_tok + (size_t)b * TC;
+    case 2: return A.s_ext + (size_t)b * ext_cap(A.B);
+    case 3: return A.s_sym + (size_t)b * TC;
+    default: return A.s_grp + (size_t)b * TC;
+  }
+}
+__device__ __forceinline__ uint32_t stream_len(const EncArgs& A, uint32_t b, uint32_t s) {
+  const uint32_t* c = A.bcnt + b * 8;
+  return s == 0 ? c[1] : s == 2 ? c[2] : s == 4 ? c[4] : c[0];
+}
+
+__global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
+  const uint32_t b = blockIdx.x, s = blockIdx.y, k = threadIdx.x, g = b * 5 + s;
+  const uint32_t ns = stream_len(A, b, s);
+  uint32_t* info = A.sinfo + (size_t)g * 4;
+  if (ns == 0) {
+    if (k == 0) { info[0] = 0; info[1] = 0; info[2] = 0; info[3] = 0; }
+    return;
+  }
+  const uint8_t* sym = stream_syms(A, b, s);
+  __shared__ uint32_t hist[256], freq[256], cum[256], red[3];
+  for (uint32_t i = k; i < 256; i += 64) hist[i] = 0;
+  __syncthreads();
+  for (uint32_t i = k; i < ns; i += 64) atomicAdd(&hist[sym[i]], 1u);
+  __syncthreads();
+  // normalisation (src/codec.h:41-66) by warp 0: lane l holds symbols 8l .. 8l+7
+  if (k < 32) {
+    uint32_t f[8], sum = 0, np = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t c = hist[k * 8 + q];
+      f[q] = c ? max(1u, (uint32_t)(((uint64_t)c << kScaleBits) / ns)) : 0u;
+      sum += f[q];
+      np += c != 0;
+    }
+    sum = warp_sum(sum);
+    np = warp_sum(np);
+    // too many: one from the largest frequency above 1 (the lowest symbol on a tie), repeatedly
+    while (sum > kScale) {
+      uint32_t bv = 0, bi = 0xFFFFFFFFu;
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (f[q] > 1 && f[q] > bv) { bv = f[q]; bi = k * 8 + q; }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const uint32_t ov = __shfl_xor_sync(kFull, bv, o), oi = __shfl_xor_sync(kFull, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if ((bi >> 3) == k) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) if ((uint32_t)q == (bi & 7u)) --f[q];
+      }
+      --sum;
+    }
+    if (sum < kScale) {  // too few: the deficit to the largest (the lowest symbol on a tie)
+      uint32_t bv = f[0], bi = k * 8;
+#pragma unroll
+      for (int q = 1; q < 8; ++q)
+        if (f[q] > bv) { bv = f[q]; bi = k * 8 + q; }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const uint32_t ov = __shfl_xor_sync(kFull, bv, o), oi = __shfl_xor_sync(kFull, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if ((bi >> 3) == k) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) if ((uint32_t)q == (bi & 7u)) f[q] += kScale - sum;
+      }
+    }
+    uint32_t tot = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) tot += f[q];
+    uint32_t c0 = warp_incl_scan(tot) - tot;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      freq[k * 8 + q] = f[q];
+      cum[k * 8 + q] = c0;
+      A.freq[(size_t)g * 256 + k * 8 + q] = (uint16_t)f[q];
+      c0 += f[q];
+    }
+    if (k == 0) red[0] = np;
+  }
+  __syncthreads();
+  // lane k codes symbols k, k+64, ... last first, backwards into its scratch (src/codec.h:112-128)
+  const uint32_t LC = lane_cap(A.B, s);
+  uint8_t* end = A.lanes + (size_t)b * lanes_per_block(A.B) + lane_base(A.B, s) + (size_t)(k + 1) * LC;
+  uint8_t* ptr = end;
+  uint32_t x = kRansLow;
+  if (k < ns) {
+    for (int64_t i = k + (int64_t)((ns - 1 - k) / kLanes) * kLanes; i >= 0; i -= kLanes) {
+      const uint32_t c = sym[i], f = freq[c];
+      const uint32_t xmax = f << (23 - kScaleBits + 8);
+      while (x >= xmax) { *--ptr = (uint8_t)x; x >>= 8; }
+      x = ((x / f) << kScaleBits) + (x % f) + cum[c];
+    }
+  }
+  ptr -= 4;
+  st32(ptr, x);
+  const uint32_t ll = (uint32_t)(end - ptr);
+  A.lanelen[(size_t)g * kLanes + k] = ll;
+  const uint32_t lsum = warp_sum(ll);
+  if (lane_id() == 0) red[1 + (k >> 5)] = lsum;
+  __syncthreads();
+  if (k == 0) {
+    const uint32_t np = red[0];
+    const uint32_t total = 32 + 2 * np + 4 * kLanes + red[1] + red[2];
+    const uint32_t kind = total >= ns ? 0u : 1u;  // raw when rANS is not smaller (src/codec.h:130)
+    info[0] = kind;
+    info[1] = kind ? total : ns;
+    info[2] = np;
+    info[3] = ns;
+  }
+}
+
+// ---------------------------------------------------------------- 6. the payload
+__global__ void __launch_bounds__(256) k_enc_pack(EncArgs A) {
+  const uint32_t b = blockIdx.x, tid = threadIdx.x;
+  const uint32_t n = A.in_len[b];
+  uint32_t* c = A.bcnt + b * 8;
+  const uint32_t nob = c[3];
+  uint64_t off[6];
+  off[0] = kHdrBytes;
+  for (uint32_t s = 0; s < 5; ++s) off[s + 1] = off[s] + 5 + A.sinfo[(size_t)(b * 5 + s) * 4 + 1];
+  const uint64_t total = off[5] + nob;
+  if (total >= n) {  // stored (src/codec2.h:152, src/archive.h:394)
+    if (tid == 0) { c[5] = n; c[6] = 0; }
+    return;
+  }
+  uint8_t* o = A.slab + (size_t)b * A.B;
+  if (tid == 0) {
+    st32(o, c[0]); st32(o + 4, c[1]); st32(o + 8, c[2]); st32(o + 12, nob); st32(o + 16, c[4]);
+    c[5] = (uint32_t)total; c[6] = 1;
+  }
+  __shared__ uint32_t lofs[kLanes + 1];
+  __shared__ uint32_t wcnt[8];
+  for (uint32_t s = 0; s < 5; ++s) {
+    const uint32_t g = b * 5 + s;
+    const uint32_t* info = A.sinfo + (size_t)g * 4;
+    const uint32_t kind = info[0], len = info[1], np = info[2], ns = info[3];
+    uint8_t* d = o + off[s];
+    if (tid == 0) { d[0] = (uint8_t)kind; st32(d + 1, len); }
+    const uint8_t* sym = stream_syms(A, b, s);
+    if (kind == 0) {
+      for (uint32_t i = tid; i < ns; i += blockDim.x) d[5 + i] = sym[i];
+      continue;
+    }
+    const uint16_t* fq = A.freq + (size_t)g * 256;
+    // present bitmap, then the frequencies of the present symbols in symbol order
+    const uint32_t f = fq[tid];
+    const uint32_t pres = f != 0;
+    const unsigned bal = __ballot_sync(kFull, pres);
+    if ((tid & 7u) == 0) d[5 + (tid >> 3)] = (uint8_t)((bal >> (tid & 31u)) & 0xFFu);
+    if ((tid & 31u) == 0) wcnt[tid >> 5] = __popc(bal);
+    __syncthreads();
+    uint32_t idx = __popc(bal & ((1u << (tid & 31u)) - 1u));
+    for (uint32_t k = 0; k < (tid >> 5); ++k) idx += wcnt[k];
+    if (pres) { d[5 + 32 + 2 * idx] = (uint8_t)f; d[5 + 32 + 2 * idx + 1] = (uint8_t)(f >> 8); }
+    const uint32_t* ll = A.lanelen + (size_t)g * kLanes;
+    if (tid < kLanes) st32(d + 5 + 32 + 2 * np + 4 * tid, ll[tid]);
+    if (tid < 32) {
+      const uint32_t a = ll[2 * tid], bb = ll[2 * tid + 1];
+      const uint32_t inc = warp_incl_scan(a + bb);
+      lofs[2 * tid] = inc - a - bb;
+      lofs[2 * tid + 1] = inc - bb;
+    }
+    __syncthreads();
+    const uint32_t data0 = 5 + 32 + 2 * np + 4 * kLanes;
+    const uint32_t LC = lane_cap(A.B, s);
+    const uint8_t* lb = A.lanes + (size_t)b * lanes_per_block(A.B) + lane_base(A.B, s);
+    for (uint32_t jl = tid >> 5; jl < kLanes; jl += blockDim.x >> 5) {
+      const uint32_t len_j = ll[jl];
+      const uint8_t* srcp = lb + (size_t)(jl + 1) * LC - len_j;
+      uint8_t* dst = d + data0 + lofs[jl];
+      for (uint32_t i = lane_id(); i < len_j; i += 32) dst[i] = srcp[i];
+    }
+    __syncthreads();
+  }
+  const uint8_t* bits = A.s_bits + (size_t)b * bits_cap(A.B);
+  for (uint32_t i = tid; i < nob; i += blockDim.x) o[off[5] + i] = bits[i];
+}
+
+// ---------------------------------------------------------------- 7. record bodies back to back
+__global__ void __launch_bounds__(1024) k_enc_scan(EncArgs A) {
+  const uint32_t tid = threadIdx.x, nb = A.nb;
+  const uint32_t per = (nb + 1023) / 1024;
+  const uint32_t b0 = min(tid * per, nb), b1 = min(b0 + per, nb);
+  uint64_t sum = 0;
+  for (uint32_t b = b0; b < b1; ++b) {
+    const uint32_t* c = A.bcnt + b * 8;
+    sum += c[6] ? c[5] : (A.emit_stored ? A.in_len[b] : 0u);
+  }
+  __shared__ uint64_t ws[32];
+  uint64_t incl = sum;
+  const uint32_t l = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t t = __shfl_up_sync(kFull, incl, o);
+    if (l >= (uint32_t)o) incl += t;
+  }
+  if (l == 31) ws[tid >> 5] = incl;
+  __syncthreads();
+  if (tid < 32) {
+    uint64_t v = ws[tid], x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t t = __shfl_up_sync(kFull, x, o);
+      if (l >= (uint32_t)o) x += t;
+    }
+    ws[tid] = x - v;
+  }
+  __syncthreads();
+  uint64_t off = ws[tid >> 5] + incl - sum;
+  for (uint32_t b = b0; b < b1; ++b) {
+    const uint32_t* c = A.bcnt + b * 8;
+    const uint32_t method = c[6];
+    const uint32_t len = method ? c[5] : A.in_len[b];
+    A.out_off[b] = off;
+    A.out_len[b] = len;
+    A.out_method[b] = (uint8_t)method;
+    off += method ? len : (A.emit_stored ? len : 0u);
+  }
+  if (tid == 1023) *A.out_total = off;
+}
+
+__global__ void __launch_bounds__(256) k_enc_emit(EncArgs A) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t method = A.bcnt[b * 8 + 6];
+  if (!method && !A.emit_stored) return;
+  const uint64_t off = A.out_off[b];
+  const uint32_t len = A.out_len[b];
+  if (off + len > A.out_cap) return;  // (the host checks out_total against out_cap)
+  const uint8_t* s = method ? A.slab + (size_t)b * A.B : A.in + A.in_off[b];
+  uint8_t* d = A.out + off;
+  uint32_t i = 0;
+  if ((((uintptr_t)d ^ (uintptr_t)s) & 15u) == 0) {
+    const uint32_t head = min(len, (uint32_t)((16u - ((uintptr_t)d & 15u)) & 15u));
+    if (threadIdx.x < head) d[threadIdx.x] = s[threadIdx.x];
+    i = head;
+    const uint32_t nvec = (len - i) / 16;
+    for (uint32_t v = threadIdx.x; v < nvec; v += blockDim.x)
+      reinterpret_cast<uint4*>(d + i)[v] = reinterpret_cast<const uint4*>(s + i)[v];
+    i += nvec * 16;
+  }
+  for (uint32_t k = i + threadIdx.x; k < len; k += blockDim.x) d[k] = s[k];
+}
+
+void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Stages& S) {
+  if (!A.nb) return;
+  launch_crc(crc_in, st, S, "k_crc_in");
+  S.begin("k_enc_sort", st);
+  k_enc_sort<<<A.nb, 1024, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_enc_match", st);
+  k_enc_match<<<dim3((A.B + 255) / 256, A.nb), 256, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_enc_parse", st);
+  k_enc_parse<<<A.nb, 256, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_enc_streams", st);
+  k_enc_streams<<<(A.nb + 3) / 4, 128, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_enc_rans", st);
+  k_enc_rans<<<dim3(A.nb, 5), 64, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_enc_pack", st);
+  k_enc_pack<<<A.nb, 256, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_enc_scan", st);
+  k_enc_scan<<<1, 1024, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_enc_emit", st);
+  k_enc_emit<<<A.nb, 256, 0, st>>>(A);
+  S.end(st);
+}
+
+}  // namespace zc

@@ -1,0 +1,102 @@
+// zc_kernels.h -- argument blocks and launchers of the ZB2 kernels (host and device view).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace zc {
+
+struct CrcTables;
+
+// kernel launch accounting and optional per-stage timing with CUDA events on the launching stream
+// (the counterpart of the reference's ZERO_PROFILE stage timer, src/gpu_codec.h:32-49, without its
+// device syncs).  Implemented in zc_api.cu.
+struct Stages {
+  bool timing = false;
+  uint64_t launches = 0;
+  void* impl = nullptr;  // the context's event records
+  void begin(const char* name, cudaStream_t st);  // call before a kernel launch
+  void end(cudaStream_t st);                      // and after it
+};
+
+// ---- decoder
+struct DecMeta {  // per block: the payload's counts and where its offset bits start
+  uint32_t nt, nl, ne, nob, ng, bits_off;
+};
+
+struct DecArgs {
+  const uint8_t* comp;        // payloads
+  const uint64_t* comp_off;   // per block
+  const uint32_t* comp_len;
+  const uint8_t* method;
+  const uint32_t* raw_len;
+  uint32_t nb, B;
+  uint8_t* out;               // raw bytes of block b at out + out_off[b]
+  const uint64_t* out_off;
+  uint32_t* err;              // per block status (zeroed before)
+  // scratch, per block slot b: lit at b*B, tok / sym / grp at b*tok_cap(B), ext at b*ext_cap(B)
+  uint8_t *s_lit, *s_tok, *s_sym, *s_grp, *s_ext;
+  DecMeta* meta;
+};
+
+struct CrcArgs {
+  const uint8_t* base;
+  const uint64_t* offs;
+  const uint32_t* lens;
+  uint32_t nb;
+  uint32_t* crc;              // out, per block
+  uint32_t* err;              // optional: blocks with err != 0 are skipped; with expect, a mismatch sets E_CRC
+  const uint32_t* expect;     // optional
+  const CrcTables* tables;
+};
+
+void launch_decode(const DecArgs& A, cudaStream_t st, Stages& S);
+void launch_crc(const CrcArgs& A, cudaStream_t st, Stages& S, const char* name);
+
+// ---- encoder
+struct EncArgs {
+  const uint8_t* in;          // block b: in_len[b] bytes at in + in_off[b]; >= 16 readable bytes after the last
+  const uint64_t* in_off;
+  const uint32_t* in_len;
+  uint32_t nb, B, block_log;
+  int depth;                  // hash chain steps (8 / 32 / 256)
+  uint32_t cmp_cap;           // bytes the all-position match pass compares before deferring to the parse
+  // scratch, per block slot (capacity B positions)
+  uint32_t *tmp_pos, *srt_pos, *rank, *minfo;
+  uint16_t *tmp_h, *srt_h;
+  uint32_t *tk_i, *tk_m, *tk_d;   // tokens, tok_cap(B) per block
+  uint32_t* bcnt;                 // per block [8]: nt, nl, ne, nob, ng, payload size, method
+  uint8_t *s_lit, *s_tok, *s_ext, *s_sym, *s_grp, *s_bits;
+  uint8_t* lanes;                 // rANS lane scratch, lanes_per_block(B) per block
+  uint16_t* freq;                 // per (block, stream) 256
+  uint32_t* lanelen;              // per (block, stream) 64
+  uint32_t* sinfo;                // per (block, stream) 4: kind, section body length, present symbols, symbols
+  uint8_t* slab;                  // per block B bytes: the payload when it is smaller than the block
+  // output
+  uint8_t* out;                   // record bodies packed back to back
+  uint64_t out_cap;
+  uint64_t* out_off;              // per block
+  uint32_t* out_len;              // per block: payload length (raw length when stored)
+  uint8_t* out_method;            // per block
+  uint64_t* out_total;            // device u64: bytes written to out
+  int emit_stored;                // 1: copy stored blocks' raw bytes into out as well
+};
+
+// lane scratch layout per block: stream s starts at lane_base(s), each of its 64 lanes has lane_cap(s)
+// bytes (rANS emits at most 2 bytes per symbol plus a 4-byte flush)
+__host__ __device__ inline uint32_t stream_cap(uint32_t B, uint32_t s) {
+  return s == 0 ? B : s == 2 ? B / 5 + 64 : B / 4 + 16;
+}
+__host__ __device__ inline uint32_t lane_cap(uint32_t B, uint32_t s) {
+  return 2 * ((stream_cap(B, s) + 63) / 64) + 16;
+}
+__host__ __device__ inline uint64_t lane_base(uint32_t B, uint32_t s) {
+  uint64_t o = 0;
+  for (uint32_t k = 0; k < s; ++k) o += 64ull * lane_cap(B, k);
+  return o;
+}
+__host__ __device__ inline uint64_t lanes_per_block(uint32_t B) { return lane_base(B, 5); }
+__host__ __device__ inline uint32_t bits_cap(uint32_t B) { return 5 * B / 8 + 64; }
+
+void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Stages& S);
+
+}  // namespace zc

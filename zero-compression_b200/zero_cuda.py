@@ -1,0 +1,267 @@
+"""Python binding of the B200 ZB2 block codec (ctypes over libzero_cuda.so, the C ABI of include/zero_cuda.h).
+
+It mirrors the reference's codec interface ``zero::Codec`` (src/archive.h:45-69):
+
+    codec = CudaCodec(level=5)          # GpuCodec + choose_codec, src/main.cpp:36-57 / src/gpu_codec.h:63-86
+    outs = codec.compress(data, 18)     # -> [BlockOut(method, data)], one per block (src/archive.h:60)
+    raw = codec.decompress(blocks)      # [BlockIn(method, raw_len, data)] -> raw bytes (src/archive.h:63)
+    codec.batch_bytes(18), codec.batch_bytes_decode(18), codec.prepare(18), codec.name()
+
+Errors follow the reference's split (src/safe_codec.h:36-49): ``DataError`` for damaged input (zb::Error:
+the caller may retry on a CPU codec, which reports what is wrong) and ``DeviceError`` for a failed GPU
+(gpu::Error).  There is no CPU path here: without the built library or a CUDA device every call raises.
+"""
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(HERE, "libzero_cuda.so")
+
+ZC_OK, ZC_E_DATA, ZC_E_DEVICE, ZC_E_NOMEM, ZC_E_ARG = 0, 1, 2, 3, 4
+STORED, ZB2 = 0, 1
+
+_u8p = C.POINTER(C.c_uint8)
+_u32p = C.POINTER(C.c_uint32)
+_u64p = C.POINTER(C.c_uint64)
+_vp = C.c_void_p
+
+
+class ZcError(RuntimeError):
+    code = -1
+
+
+class DataError(ZcError):
+    """Damaged input or an impossible result (the reference's zb::Error)."""
+    code = ZC_E_DATA
+
+
+class DeviceError(ZcError):
+    """The GPU failed (the reference's gpu::Error)."""
+    code = ZC_E_DEVICE
+
+
+class NoMemError(DeviceError):
+    code = ZC_E_NOMEM
+
+
+class ArgError(ZcError, ValueError):
+    code = ZC_E_ARG
+
+
+_lib = None
+
+
+def lib():
+    """The loaded C library; raises when it was not built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO):
+            raise ImportError(f"{SO} is not built: run __graft_entry__.build() (make -C zero-compression_b200/csrc)")
+        L = C.CDLL(SO)
+        L.zc_open.argtypes = [C.POINTER(_vp), C.c_int]
+        L.zc_close.argtypes = [_vp]
+        L.zc_last_error.argtypes = [_vp]
+        L.zc_last_error.restype = C.c_char_p
+        L.zc_name.argtypes = [_vp]
+        L.zc_name.restype = C.c_char_p
+        L.zc_prepare.argtypes = [_vp, C.c_uint32, C.c_int]
+        L.zc_batch_bytes.argtypes = [_vp, C.c_uint32]
+        L.zc_batch_bytes.restype = C.c_size_t
+        L.zc_batch_bytes_decode.argtypes = [_vp, C.c_uint32]
+        L.zc_batch_bytes_decode.restype = C.c_size_t
+        L.zc_compress.argtypes = [_vp, _vp, C.c_size_t, C.c_uint32, C.c_int, _vp, _vp, _vp, _vp, C.c_size_t, _vp]
+        L.zc_compress_batch.argtypes = [_vp, _vp, _vp, _vp, C.c_uint32, C.c_uint32, C.c_int, _vp, _vp, _vp, _vp,
+                                        C.c_size_t, _vp]
+        L.zc_decompress.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, C.c_uint32, _vp, _vp, _vp]
+        L.zc_compress_device.argtypes = [_vp, _vp, _vp, _vp, C.c_uint32, C.c_uint32, C.c_int, _vp, _vp, _vp, _vp,
+                                         C.c_size_t, _vp, _vp, _vp]
+        L.zc_decompress_device.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp,
+                                           _vp]
+        L.zc_crc32.argtypes = [_vp, _vp, C.c_size_t, _u32p]
+        L.zc_crc32_combine.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64]
+        L.zc_crc32_combine.restype = C.c_uint32
+        L.zc_launch_count.argtypes = [_vp]
+        L.zc_launch_count.restype = C.c_uint64
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def _as_u8(data):
+    if isinstance(data, np.ndarray):
+        return np.ascontiguousarray(data.reshape(-1).view(np.uint8))
+    return np.frombuffer(data, np.uint8)
+
+
+@dataclass
+class BlockOut:
+    """One compressed block (src/archive.h:46-49): method 0 stored (the caller writes the input), 1 ZB2."""
+    method: int = STORED
+    data: bytes = b""
+
+
+@dataclass
+class BlockIn:
+    """One block to decode (src/archive.h:50-55)."""
+    method: int = STORED
+    raw_len: int = 0
+    data: bytes = b""
+
+    @property
+    def comp_len(self):
+        return len(self.data)
+
+
+def _raise(ctx, rc):
+    msg = lib().zc_last_error(ctx).decode(errors="replace") if ctx else "zc_open failed"
+    cls = {ZC_E_DATA: DataError, ZC_E_DEVICE: DeviceError, ZC_E_NOMEM: NoMemError, ZC_E_ARG: ArgError}.get(rc, ZcError)
+    raise cls(msg)
+
+
+class CudaCodec:
+    """The GPU codec behind the reference's zero::Codec interface, on a CUDA device (sm_100a)."""
+
+    def __init__(self, level=5, device=0):
+        self.level = level
+        ctx = _vp()
+        rc = lib().zc_open(C.byref(ctx), device)
+        self._ctx = ctx
+        if rc:
+            msg = lib().zc_last_error(ctx).decode(errors="replace") if ctx else "zc_open failed"
+            self.close()
+            raise DeviceError(msg)
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_ctx", None):
+            lib().zc_close(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc:
+            _raise(self._ctx, rc)
+
+    # -- zero::Codec
+    def name(self):
+        return lib().zc_name(self._ctx).decode()
+
+    def batch_bytes(self, block_log):
+        return lib().zc_batch_bytes(self._ctx, block_log)
+
+    def batch_bytes_decode(self, block_log):
+        return lib().zc_batch_bytes_decode(self._ctx, block_log)
+
+    def prepare(self, block_log):
+        self._check(lib().zc_prepare(self._ctx, block_log, self.level))
+
+    def launch_count(self):
+        return lib().zc_launch_count(self._ctx)
+
+    def compress_arrays(self, data, block_log, level=None):
+        """n bytes in blocks of 2^block_log -> (methods, comp_lens, crcs, payloads, pay_offs) as arrays."""
+        a = _as_u8(data)
+        B = 1 << block_log
+        nb = (a.size + B - 1) // B
+        methods = np.zeros(max(nb, 1), np.uint8)
+        lens = np.zeros(max(nb, 1), np.uint32)
+        crcs = np.zeros(max(nb, 1), np.uint32)
+        offs = np.zeros(max(nb, 1), np.uint64)
+        pay = np.empty(max(a.size, 1), np.uint8)
+        self._check(lib().zc_compress(self._ctx, _ptr(a), a.size, block_log, self.level if level is None else level,
+                                      _ptr(methods), _ptr(lens), _ptr(crcs), _ptr(pay), pay.size, _ptr(offs)))
+        return methods[:nb], lens[:nb], crcs[:nb], pay, offs[:nb]
+
+    def compress_batch_arrays(self, data, in_offs, in_lens, block_log, level=None):
+        """Blocks of uneven sizes (block b: in_lens[b] bytes at data[in_offs[b]:]) in one launch per stage."""
+        a = _as_u8(data)
+        offs_in = np.ascontiguousarray(in_offs, np.uint64)
+        lens_in = np.ascontiguousarray(in_lens, np.uint32)
+        nb = offs_in.size
+        methods = np.zeros(max(nb, 1), np.uint8)
+        lens = np.zeros(max(nb, 1), np.uint32)
+        crcs = np.zeros(max(nb, 1), np.uint32)
+        offs = np.zeros(max(nb, 1), np.uint64)
+        pay = np.empty(max(int(lens_in.sum()), 1), np.uint8)
+        self._check(lib().zc_compress_batch(self._ctx, _ptr(a), _ptr(offs_in), _ptr(lens_in), nb, block_log,
+                                            self.level if level is None else level, _ptr(methods), _ptr(lens),
+                                            _ptr(crcs), _ptr(pay), pay.size, _ptr(offs)))
+        return methods[:nb], lens[:nb], crcs[:nb], pay, offs[:nb]
+
+    def compress(self, data, block_log):
+        """zero::Codec::compress: one BlockOut per block; a stored block carries no data."""
+        methods, lens, _, pay, offs = self.compress_arrays(data, block_log)
+        return [BlockOut(int(m), pay[int(o): int(o) + int(l)].tobytes() if m else b"")
+                for m, l, o in zip(methods, lens, offs)]
+
+    def decompress_arrays(self, comp, comp_offs, comp_lens, methods, raw_lens, raise_on_damage=True):
+        """Blocks as arrays -> (raw bytes, per-block CRC-32s, per-block status)."""
+        comp = _as_u8(comp)
+        comp_offs = np.ascontiguousarray(comp_offs, np.uint64)
+        comp_lens = np.ascontiguousarray(comp_lens, np.uint32)
+        methods = np.ascontiguousarray(methods, np.uint8)
+        raw_lens = np.ascontiguousarray(raw_lens, np.uint32)
+        nb = raw_lens.size
+        out = np.empty(max(int(raw_lens.sum()), 1), np.uint8)
+        crcs = np.zeros(max(nb, 1), np.uint32)
+        errs = np.zeros(max(nb, 1), np.uint32)
+        rc = lib().zc_decompress(self._ctx, _ptr(comp), _ptr(comp_offs), _ptr(comp_lens), _ptr(methods),
+                                 _ptr(raw_lens), nb, _ptr(out), _ptr(crcs), _ptr(errs))
+        if rc and (rc != ZC_E_DATA or raise_on_damage):
+            _raise(self._ctx, rc)
+        return out[: int(raw_lens.sum())], crcs[:nb], errs[:nb]
+
+    def decompress(self, blocks):
+        """zero::Codec::decompress: the blocks' raw bytes, one after the other."""
+        if not blocks:
+            return b""
+        datas = [bytes(b.data) for b in blocks]
+        comp = np.frombuffer(b"".join(datas) or b"\0", np.uint8)
+        lens = np.array([len(d) for d in datas], np.uint64)
+        offs = np.concatenate([[0], np.cumsum(lens)[:-1]]).astype(np.uint64)
+        out, _, _ = self.decompress_arrays(comp, offs, lens, [b.method for b in blocks], [b.raw_len for b in blocks])
+        return out.tobytes()
+
+    def crc32(self, data):
+        a = _as_u8(data)
+        v = C.c_uint32()
+        self._check(lib().zc_crc32(self._ctx, _ptr(a), a.size, C.byref(v)))
+        return v.value
+
+    # -- device-resident forms (torch CUDA tensors; work queued on `stream`, a raw cudaStream_t handle)
+    def compress_device(self, d_in, d_in_offs, d_in_lens, nb, block_log, d_methods, d_lens, d_crcs, d_out,
+                        d_out_offs, d_total, stream=0, level=None):
+        self._check(lib().zc_compress_device(
+            self._ctx, d_in.data_ptr(), d_in_offs.data_ptr(), d_in_lens.data_ptr(), nb, block_log,
+            self.level if level is None else level, d_methods.data_ptr(), d_lens.data_ptr(),
+            d_crcs.data_ptr() if d_crcs is not None else None, d_out.data_ptr(), d_out.numel(),
+            d_out_offs.data_ptr(), d_total.data_ptr(), stream or None))
+
+    def decompress_device(self, d_comp, d_comp_offs, d_comp_lens, d_methods, d_raw_lens, nb, block_log, d_out,
+                          d_out_offs, d_crcs, d_err, stream=0):
+        self._check(lib().zc_decompress_device(
+            self._ctx, d_comp.data_ptr(), d_comp_offs.data_ptr(), d_comp_lens.data_ptr(), d_methods.data_ptr(),
+            d_raw_lens.data_ptr(), nb, block_log, d_out.data_ptr(), d_out_offs.data_ptr(),
+            d_crcs.data_ptr() if d_crcs is not None else None, d_err.data_ptr(), stream or None))
+
+
+def crc32_combine(a, b, len_b):
+    """crc32::combine (src/crc32.h:60-66) on the host."""
+    return lib().zc_crc32_combine(a, b, len_b)
