@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 ZB2 block codec: compress then extract (a bit-exact round trip) of 1 GiB of
+LZ-structured synthetic data per GPU at block 2^18 (256 KiB) and level 5.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python -m torch.distributed.run --nproc-per-node N --master-addr 127.0.0.1 bench.py --gpus N ...
+
+One step = compress the whole input (one launch per stage per 256 MiB of blocks) and decompress the
+result, all device-resident: `value` is raw GB / step time over every rank (max over ranks of the device
+time).  `e2e` is the same round trip through the host C ABI (zc_compress / zc_decompress) with pinned host
+buffers, copies included.  Per-kernel CUDA-event times give the dominant kernel's roofline against the
+measured HBM bandwidth; the reference CPU codec (oracle/_ref, all host threads) is timed on a sample.
+
+Blocks are independent, so N GPUs each code their own 1 GiB (weak scaling, no collective on the data
+path; a barrier and a max-reduction of the timings only).
+
+--impl reference times the reference's own CPU codec (CpuCodec of src/archive.h, compiled from the
+reference sources into oracle/_ref/libzref.so; the C restatement oracle/liboracle.so when that is absent)
+on a bounded sample of the same workload, on rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "zero-compression_b200"))
+
+METRIC = "compress/decompress GB/s on 1 B200, bit-exact round-trip; served p50/p99 latency"
+GB = 1e9
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_data(n, block_log, seed):
+    import datagen as G
+    return G.lz_mix(n, block_log, seed)
+
+
+def cpu_round_trip(data, block_log, level):
+    """One round trip of `data` through the reference CPU codec (all threads); returns (seconds, kind, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    B = 1 << block_log
+    if O.Ref.available():
+        t0 = time.perf_counter()
+        methods, lens, pays = O.Ref.cpu_compress(data, block_log, O.depth_for_level(level))
+        comp, offs, at = [], [], 0
+        for b in range(len(methods)):
+            blk = data[b * B:(b + 1) * B]
+            c = pays[b] if methods[b] else blk.tobytes()
+            comp.append(c)
+            offs.append(at)
+            at += len(c)
+        raw_lens = [min(B, data.size - b * B) for b in range(len(methods))]
+        blob = np.frombuffer(b"".join(comp), np.uint8)
+        out = O.Ref.cpu_decompress(blob, offs, [len(c) for c in comp], methods, raw_lens)
+        dt = time.perf_counter() - t0
+        assert np.array_equal(out, data), "reference CPU round trip differs"
+        return dt, "reference", O.Ref.hardware_threads()
+    if not O.Port.available():
+        O.build()
+    t0 = time.perf_counter()
+    for o in range(0, data.size, B):
+        blk = data[o:o + B].tobytes()
+        pay = O.Port.compress_block(blk, O.depth_for_level(level))
+        if len(pay) < len(blk):
+            assert O.Port.decompress_block(pay, len(blk)) == blk
+    return time.perf_counter() - t0, "port", 1
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    B = 1 << args.block
+    sample = min(args.size_mib << 20, 256 << 20)
+    data = make_data(sample, args.block, 1000)
+    times = []
+    kind, cores = "reference", 1
+    for i in range(args.warmup + args.steps):
+        dt, kind, cores = cpu_round_trip(data, args.block, args.level)
+        if i >= args.warmup:
+            times.append(dt)
+    t = statistics.mean(times)
+    value = sample / t / GB
+    desc = f"{sample >> 20} MiB of the lz_mix workload (block {B >> 10} KiB, level {args.level}), round trip per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded lz_mix generator)",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": cores, "kind": kind, "sample": desc},
+        "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args):
+    return {"workload": f"lz_mix {args.size_mib} MiB per GPU, block {args.block} ({(1 << args.block) >> 10} KiB), "
+                        f"level {args.level}: compress then extract (bit-exact round trip)",
+            "block_log": args.block, "level": args.level, "bytes_per_gpu": args.size_mib << 20,
+            "generator": "literal runs geometric(mean 8) over geometric(p=0.05) symbols; matches log-uniform "
+                         "length [4,258], offset log-uniform [1, block]",
+            "l2_flush": "none needed: 1 GiB of input per GPU is larger than the 126 MB L2",
+            "parallelism": f"dp{args.gpus} (independent blocks per GPU)"}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import zero_cuda as Z
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    bl, level = args.block, args.level
+    B = 1 << bl
+    n = args.size_mib << 20
+    nb = (n + B - 1) // B
+    host = make_data(n, bl, 1000 + rank)
+    pinned = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = host
+    codec = Z.CudaCodec(level=level, device=local)
+    per = codec.batch_bytes(bl) // B  # blocks per launch
+
+    d_in = torch.zeros(n + 64, dtype=torch.uint8, device=dev)
+    d_in[:n].copy_(pinned, non_blocking=False)
+    offs = torch.arange(nb, dtype=torch.int64, device=dev) * B
+    lens = torch.clamp(n - offs, max=B).to(torch.int32)
+    d_out = torch.empty(n + 64, dtype=torch.uint8, device=dev)
+    d_dec = torch.empty(n + 64, dtype=torch.uint8, device=dev)
+    methods = torch.zeros(nb, dtype=torch.uint8, device=dev)
+    clens = torch.zeros(nb, dtype=torch.int32, device=dev)
+    crcs = torch.zeros(nb, dtype=torch.int32, device=dev)
+    dcrcs = torch.zeros(nb, dtype=torch.int32, device=dev)
+    errs = torch.zeros(nb, dtype=torch.int32, device=dev)
+    ooffs = torch.zeros(nb, dtype=torch.int64, device=dev)
+    totals = torch.zeros((nb + per - 1) // per, dtype=torch.int64, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    chunks = [(b0, min(per, nb - b0)) for b0 in range(0, nb, per)]
+
+    def compress():
+        for ci, (b0, k) in enumerate(chunks):
+            o = b0 * B
+            codec.compress_device(d_in, offs[b0:], lens[b0:], k, bl, methods[b0:], clens[b0:], crcs[b0:],
+                                  d_out[o:o + k * B + 64], ooffs[b0:], totals[ci:], stream=sh)
+
+    def decompress():
+        for ci, (b0, k) in enumerate(chunks):
+            o = b0 * B
+            codec.decompress_device(d_out[o:o + k * B + 64], ooffs[b0:], clens[b0:], methods[b0:], lens[b0:], k, bl,
+                                    d_dec, offs[b0:], dcrcs[b0:], errs[b0:], stream=sh)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    # warm-up (untimed)
+    for _ in range(args.warmup):
+        compress()
+        decompress()
+    torch.cuda.synchronize(dev)
+    comp_bytes = int(totals.sum().item())
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    codec.profile(True)
+    launches0 = codec.launch_count()
+    barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                ev[i][0].record(stream)
+                compress()
+                ev[i][1].record(stream)
+                decompress()
+                ev[i][2].record(stream)
+        torch.cuda.synchronize(dev)
+    barrier()
+    launches = codec.launch_count() - launches0
+    stages = codec.profile_stages()
+    codec.profile(False)
+    t_c = [ev[i][0].elapsed_time(ev[i][1]) for i in range(args.steps)]
+    t_d = [ev[i][1].elapsed_time(ev[i][2]) for i in range(args.steps)]
+    tot_ms = ev[0][0].elapsed_time(ev[-1][2])
+    local_times = torch.tensor([tot_ms, sum(t_c), sum(t_d)], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(local_times, op=dist.ReduceOp.MAX)
+    tot_ms, sum_c, sum_d = local_times.tolist()
+
+    # bit-exact round trip and CRCs
+    ok = bool(torch.equal(d_dec[:n], d_in[:n])) and bool(torch.equal(dcrcs, crcs)) and int(errs.abs().sum()) == 0
+    flags = torch.tensor([0 if ok else 1], device=dev)
+    if ws > 1:
+        dist.all_reduce(flags, op=dist.ReduceOp.MAX)
+    ok = int(flags.item()) == 0
+
+    ms_per_step = tot_ms / args.steps
+    value = ws * n / (ms_per_step * 1e-3) / GB
+    comp_gbs = ws * n / (sum_c / args.steps * 1e-3) / GB
+    dec_gbs = ws * n / (sum_d / args.steps * 1e-3) / GB
+
+    # the dominant kernel: most time in the timed region; its algorithmic bytes are the codec's
+    # (raw + compressed) bytes of the blocks one launch covers
+    peak, peak_kind = peaks()
+    dom = max(stages.items(), key=lambda kv: kv[1][0]) if stages else ("", (0.0, 1))
+    dom_name, (dom_ms, dom_launches) = dom
+    steps_bytes = (n + comp_bytes) * args.steps
+    achieved = steps_bytes / (dom_ms * 1e-3) / GB if dom_ms else 0.0
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            tr = json.load(f)
+        if dom_name in tr:
+            traffic = int(tr[dom_name]["dram_bytes_per_input_byte"] * n / max(1, dom_launches // args.steps))
+    except Exception:
+        traffic = None
+    total_stage_ms = sum(v[0] for v in stages.values()) or 1.0
+    pipe_achieved = steps_bytes / (tot_ms * 1e-3) / GB
+
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded lz_mix generator, 1 GiB per GPU)",
+        "config": workload_config(args),
+        "compress_gbs": round(comp_gbs, 4), "decompress_gbs": round(dec_gbs, 4),
+        "ratio": round(comp_bytes / n, 5), "bit_exact": ok,
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 2), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                     "algorithmic_bytes_per_launch": int((n + comp_bytes) / max(1, dom_launches // args.steps)),
+                     "avg_launch_ms": round(dom_ms / max(1, dom_launches), 4),
+                     "pipeline_frac": round(pipe_achieved / peak, 4)},
+        "stages_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in stages.items()},
+        "stage_share": {k: round(v[0] / total_stage_ms, 4) for k, v in stages.items()},
+        "gpu_launches": int(launches),
+    }
+
+    # end to end through the host C ABI with pinned buffers (rank-local wall time, max over ranks)
+    pay_p = torch.empty(n + 64, dtype=torch.uint8, pin_memory=True)
+    dec_p = torch.empty(n + 64, dtype=torch.uint8, pin_memory=True)
+    m_h = np.zeros(nb, np.uint8)
+    l_h = np.zeros(nb, np.uint32)
+    c_h = np.zeros(nb, np.uint32)
+    o_h = np.zeros(nb, np.uint64)
+    raw_lens = np.minimum(B, n - np.arange(nb, dtype=np.int64) * B).astype(np.uint32)
+    hin = pinned.numpy()
+
+    def e2e_step():
+        codec.compress_arrays(hin, bl, out=(m_h, l_h, c_h, pay_p.numpy(), o_h))
+        # the record bodies as an archive holds them: each payload, or the raw block when stored
+        # (stored blocks are appended after the payloads, as a reader would hand them over)
+        pay_total = int(l_h[m_h == 1].sum())
+        comp_offs = o_h.copy()
+        at = pay_total
+        pv = pay_p.numpy()
+        for b in np.nonzero(m_h == 0)[0]:
+            pv[at:at + raw_lens[b]] = hin[b * B: b * B + raw_lens[b]]
+            comp_offs[b] = at
+            at += int(raw_lens[b])
+        codec.decompress_arrays(pv, comp_offs, l_h, m_h, raw_lens, out=dec_p.numpy())
+        return pay_total, at
+
+    e2e = None
+    try:
+        for _ in range(1):
+            e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            pay_total, body_total = e2e_step()
+        dt = (time.perf_counter() - t0) / args.steps
+        dts = torch.tensor([dt], dtype=torch.float64, device=dev)
+        if ws > 1:
+            dist.all_reduce(dts, op=dist.ReduceOp.MAX)
+        dt = float(dts.item())
+        same = bool(np.array_equal(dec_p.numpy()[:n], hin))
+        # compress: n bytes up, per-block records (17 B) and payloads down; decompress: the record bodies
+        # and a 33-byte block table up, n bytes and per-block CRC + status (8 B) down
+        e2e = {"value": round(ws * n / dt / GB, 4), "unit": "GB/s",
+               "h2d_bytes_per_step": int(n + body_total + nb * 33), "d2h_bytes_per_step": int(pay_total + n + nb * 25),
+               "bit_exact": same, "path": "zc_compress + zc_decompress, pinned host buffers"}
+    except Exception as e:  # reported, never hidden
+        e2e = {"value": None, "unit": "GB/s", "error": str(e)[:200]}
+    line["e2e"] = e2e
+    line["clocks"] = clk.summary()
+
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        sample = host[: min(n, 256 << 20)]
+        reps, t_cpu, kind, cores = 0, 0.0, "reference", 1
+        while reps < 1 or (t_cpu < 5.0 and reps < 8):
+            dt, kind, cores = cpu_round_trip(sample, bl, level)
+            t_cpu += dt
+            reps += 1
+        line["cpu_baseline"] = {"value": round(sample.size * reps / t_cpu / GB, 4), "unit": "GB/s", "cores": cores,
+                                "kind": kind,
+                                "sample": f"{sample.size >> 20} MiB of the same input, compress + decompress, "
+                                          f"{reps} round trip(s), block {B >> 10} KiB, level {level}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    codec.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0 if ok else 1
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--block", type=int, default=18)
+    ap.add_argument("--level", type=int, default=5)
+    ap.add_argument("--size-mib", type=int, default=1024)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

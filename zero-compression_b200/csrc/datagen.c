@@ -45,23 +45,32 @@ static uint64_t rng_geometric(zg_rng *r, double mean) {
   const double q = 1.0 - 1.0 / mean;
   return 1 + (uint64_t)floor(log(rng_unit(r)) / log(q));
 }
-/* log-uniform integer in [lo, hi] */
-static uint64_t rng_loguniform(zg_rng *r, double lo, double hi) {
-  const double v = exp(log(lo) + (log(hi + 1.0) - log(lo)) * (1.0 - rng_unit(r)));
+/* log-uniform integers in [lo, hi] (the bounds' logs computed once) */
+typedef struct { double lo, hi, llo, lhi; } zg_logu;
+static zg_logu logu(double lo, double hi) { zg_logu u = {lo, hi, log(lo), log(hi + 1.0)}; return u; }
+static uint64_t rng_loguniform(zg_rng *r, const zg_logu *u) {
+  const double v = exp(u->llo + (u->lhi - u->llo) * (1.0 - rng_unit(r)));
   uint64_t x = (uint64_t)floor(v);
-  if (x < (uint64_t)lo) x = (uint64_t)lo;
-  if (x > (uint64_t)hi) x = (uint64_t)hi;
+  if (x < (uint64_t)u->lo) x = (uint64_t)u->lo;
+  if (x > (uint64_t)u->hi) x = (uint64_t)u->hi;
   return x;
 }
-/* an index from a 256-entry cumulative table (scaled to 2^32) */
-static int pick_cdf(zg_rng *r, const uint64_t *cdf) {
-  const uint64_t u = rng_next(r) >> 32;
-  int lo = 0, hi = 255;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (u < cdf[mid]) hi = mid; else lo = mid + 1;
+/* a 256-entry cumulative table (scaled to 2^32) with a guide: guide[g] is the first index whose bound
+ * exceeds g << 20, so a draw starts its search there instead of at 0 */
+typedef struct { uint64_t cdf[256]; uint8_t guide[4096]; } zg_cdf;
+static void cdf_guide(zg_cdf *c) {
+  int k = 0;
+  for (int g = 0; g < 4096; ++g) {
+    while (k < 255 && c->cdf[k] <= ((uint64_t)g << 20)) ++k;
+    c->guide[g] = (uint8_t)k;
   }
-  return lo;
+}
+/* the smallest index whose bound exceeds a uniform 32-bit draw */
+static int pick_cdf(zg_rng *r, const zg_cdf *c) {
+  const uint64_t u = rng_next(r) >> 32;
+  int k = c->guide[u >> 20];
+  while (u >= c->cdf[k]) ++k;
+  return k;
 }
 static void copy_back(uint8_t *out, size_t at, size_t off, size_t len) {
   const uint8_t *src = out + at - off;
@@ -80,17 +89,18 @@ void zg_text_mix(uint8_t *out, size_t n, uint64_t seed) {
   }
   double z[256], zs = 0;
   for (int k = 0; k < 256; ++k) { z[k] = pow(k + 1.0, -1.1); zs += z[k]; }
-  uint64_t cdf[256];
+  zg_cdf cdf;
   double acc = 0;
-  for (int k = 0; k < 256; ++k) { acc += z[k]; cdf[k] = (uint64_t)(acc / zs * 4294967296.0); }
-  cdf[255] = (uint64_t)1 << 32;
+  for (int k = 0; k < 256; ++k) { acc += z[k]; cdf.cdf[k] = (uint64_t)(acc / zs * 4294967296.0); }
+  cdf.cdf[255] = (uint64_t)1 << 32;
+  cdf_guide(&cdf);
   const size_t SEG = 4096;
   size_t at = 0;
   for (size_t seg = 0; at < n; ++seg) {
     const size_t end = at + SEG < n ? at + SEG : n;
     if ((seg & 1) == 0 || at == 0) {
       while (at < end) {
-        const int w = pick_cdf(&r, cdf);
+        const int w = pick_cdf(&r, &cdf);
         for (int k = 0; k < wlen[w] && at < end; ++k) out[at++] = (uint8_t)words[w][k];
         if (at < end) out[at++] = (rng_next(&r) % 10 == 0) ? '\n' : ' ';
       }
@@ -119,19 +129,20 @@ void zg_lz_mix(uint8_t *out, size_t n, uint32_t block_log, uint64_t seed) {
   /* geometric(p = 0.05) over symbol ranks 0..255, truncated at 255 and renormalised */
   double pk[256], ps = 0;
   for (int k = 0; k < 256; ++k) { pk[k] = 0.05 * pow(0.95, k); ps += pk[k]; }
-  uint64_t cdf[256];
+  zg_cdf cdf;
   double acc = 0;
-  for (int k = 0; k < 256; ++k) { acc += pk[k]; cdf[k] = (uint64_t)(acc / ps * 4294967296.0); }
-  cdf[255] = (uint64_t)1 << 32;
-  const double B = (double)((size_t)1 << block_log);
+  for (int k = 0; k < 256; ++k) { acc += pk[k]; cdf.cdf[k] = (uint64_t)(acc / ps * 4294967296.0); }
+  cdf.cdf[255] = (uint64_t)1 << 32;
+  cdf_guide(&cdf);
+  const zg_logu ulen = logu(4.0, 258.0), uoff = logu(1.0, (double)((size_t)1 << block_log));
   size_t at = 0;
   while (at < n) {
     size_t lit = (size_t)rng_geometric(&r, 8.0);
     if (lit > n - at) lit = n - at;
-    for (size_t k = 0; k < lit; ++k) out[at++] = perm[pick_cdf(&r, cdf)];
+    for (size_t k = 0; k < lit; ++k) out[at++] = perm[pick_cdf(&r, &cdf)];
     if (at >= n) break;
-    size_t len = (size_t)rng_loguniform(&r, 4.0, 258.0);
-    size_t off = (size_t)rng_loguniform(&r, 1.0, B);
+    size_t len = (size_t)rng_loguniform(&r, &ulen);
+    size_t off = (size_t)rng_loguniform(&r, &uoff);
     if (off > at) off = at;
     if (len > n - at) len = n - at;
     copy_back(out, at, off, len);
@@ -158,8 +169,9 @@ void zg_random(uint8_t *out, size_t n, uint64_t seed) {
 void zg_file_plan(uint64_t *sizes, uint8_t *kinds, size_t count, uint64_t lo, uint64_t hi, uint64_t seed) {
   zg_rng r;
   rng_seed(&r, seed);
+  const zg_logu us = logu((double)lo, (double)hi);
   for (size_t i = 0; i < count; ++i) {
-    sizes[i] = rng_loguniform(&r, (double)lo, (double)hi);
+    sizes[i] = rng_loguniform(&r, &us);
     kinds[i] = (uint8_t)rng_range(&r, 0, 2);
   }
 }

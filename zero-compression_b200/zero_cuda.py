@@ -85,6 +85,8 @@ def lib():
         L.zc_crc32_combine.restype = C.c_uint32
         L.zc_launch_count.argtypes = [_vp]
         L.zc_launch_count.restype = C.c_uint64
+        L.zc_profile.argtypes = [_vp, C.c_int]
+        L.zc_profile_stages.argtypes = [_vp, C.c_uint32, _vp, _vp, _vp, _u32p]
         _lib = L
     return _lib
 
@@ -175,16 +177,36 @@ class CudaCodec:
     def launch_count(self):
         return lib().zc_launch_count(self._ctx)
 
-    def compress_arrays(self, data, block_log, level=None):
-        """n bytes in blocks of 2^block_log -> (methods, comp_lens, crcs, payloads, pay_offs) as arrays."""
+    def profile(self, on=True):
+        """Per-kernel CUDA-event timing on/off (clears the totals)."""
+        self._check(lib().zc_profile(self._ctx, 1 if on else 0))
+
+    def profile_stages(self):
+        """{kernel: (total ms, launches)} since profile(True), in first-launch order."""
+        n = C.c_uint32()
+        self._check(lib().zc_profile_stages(self._ctx, 0, None, None, None, C.byref(n)))
+        k = n.value
+        names = C.create_string_buffer(32 * max(k, 1))
+        ms = np.zeros(max(k, 1), np.float64)
+        cnt = np.zeros(max(k, 1), np.uint64)
+        self._check(lib().zc_profile_stages(self._ctx, k, names, _ptr(ms), _ptr(cnt), C.byref(n)))
+        raw = names.raw
+        return {raw[32 * i: 32 * i + 32].split(b"\0")[0].decode(): (float(ms[i]), int(cnt[i])) for i in range(k)}
+
+    def compress_arrays(self, data, block_log, level=None, out=None):
+        """n bytes in blocks of 2^block_log -> (methods, comp_lens, crcs, payloads, pay_offs) as arrays.
+        out: optional preallocated (methods, comp_lens, crcs, payloads, pay_offs), e.g. in pinned memory."""
         a = _as_u8(data)
         B = 1 << block_log
         nb = (a.size + B - 1) // B
-        methods = np.zeros(max(nb, 1), np.uint8)
-        lens = np.zeros(max(nb, 1), np.uint32)
-        crcs = np.zeros(max(nb, 1), np.uint32)
-        offs = np.zeros(max(nb, 1), np.uint64)
-        pay = np.empty(max(a.size, 1), np.uint8)
+        if out is not None:
+            methods, lens, crcs, pay, offs = out
+        else:
+            methods = np.zeros(max(nb, 1), np.uint8)
+            lens = np.zeros(max(nb, 1), np.uint32)
+            crcs = np.zeros(max(nb, 1), np.uint32)
+            offs = np.zeros(max(nb, 1), np.uint64)
+            pay = np.empty(max(a.size, 1), np.uint8)
         self._check(lib().zc_compress(self._ctx, _ptr(a), a.size, block_log, self.level if level is None else level,
                                       _ptr(methods), _ptr(lens), _ptr(crcs), _ptr(pay), pay.size, _ptr(offs)))
         return methods[:nb], lens[:nb], crcs[:nb], pay, offs[:nb]
@@ -211,15 +233,17 @@ class CudaCodec:
         return [BlockOut(int(m), pay[int(o): int(o) + int(l)].tobytes() if m else b"")
                 for m, l, o in zip(methods, lens, offs)]
 
-    def decompress_arrays(self, comp, comp_offs, comp_lens, methods, raw_lens, raise_on_damage=True):
-        """Blocks as arrays -> (raw bytes, per-block CRC-32s, per-block status)."""
+    def decompress_arrays(self, comp, comp_offs, comp_lens, methods, raw_lens, raise_on_damage=True, out=None):
+        """Blocks as arrays -> (raw bytes, per-block CRC-32s, per-block status).  out: optional
+        preallocated output (e.g. pinned memory) of at least sum(raw_lens) bytes."""
         comp = _as_u8(comp)
         comp_offs = np.ascontiguousarray(comp_offs, np.uint64)
         comp_lens = np.ascontiguousarray(comp_lens, np.uint32)
         methods = np.ascontiguousarray(methods, np.uint8)
         raw_lens = np.ascontiguousarray(raw_lens, np.uint32)
         nb = raw_lens.size
-        out = np.empty(max(int(raw_lens.sum()), 1), np.uint8)
+        if out is None:
+            out = np.empty(max(int(raw_lens.sum()), 1), np.uint8)
         crcs = np.zeros(max(nb, 1), np.uint32)
         errs = np.zeros(max(nb, 1), np.uint32)
         rc = lib().zc_decompress(self._ctx, _ptr(comp), _ptr(comp_offs), _ptr(comp_lens), _ptr(methods),
