@@ -8,7 +8,7 @@
 //   SafeCodec (src/safe_codec.h:10-50):  unchanged; it catches zb::Error (damaged data: the CPU redoes the
 //                                        batch and reports) and gpu::Error (device failure: CPU for good).
 //
-// The reference declares gpu::Error in src/gpu.h:20-28, which the CUDA build no longer includes; define
+// The reference declares gpu::Error in src/gpu.h:17-19, which the CUDA build no longer includes; define
 // ZERO_CUDA_DEFINE_GPU_ERROR before including this header to have it declared here.
 #pragma once
 #include <cstring>
