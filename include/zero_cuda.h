@@ -107,6 +107,24 @@ int zc_decompress_device(zc_ctx *ctx, const uint8_t *d_comp, const uint64_t *d_c
                          const uint8_t *d_methods, const uint32_t *d_raw_lens, uint32_t nb, uint32_t block_log,
                          uint8_t *d_out, const uint64_t *d_out_offs, uint32_t *d_crcs, uint32_t *d_err, void *stream);
 
+/* Decompression that allocates no device memory.  No counterpart in the reference: it exists for callers
+ * that cannot call cudaMalloc -- a plugin in a host process that budgets all device memory itself (an
+ * admission-controlled server, a framework that owns its allocator), or a latency-bound path where
+ * cudaMalloc / cudaFree would synchronise the device and stall other streams.  Arguments and results are
+ * those of zc_decompress_device (all device pointers, work queued on `stream`), without a context.
+ * Scratch is one fixed __device__ array of ZC_NOALLOC_SCRATCH_BYTES inside the library, held by every GPU
+ * that loads the library until the process exits.  A block of 2^b bytes needs 2^b + 3*(2^b/4 + 16) +
+ * (2^b/5 + 64) bytes of it (each part rounded up to 256, plus 256): at most 64 blocks of 64 KiB, 16 of
+ * 256 KiB or 4 of 1 MiB per call; more returns ZC_E_ARG and touches nothing.
+ * The first call on a device sets that device up (it looks up the arrays' device addresses and fills the
+ * CRC tables, with the device current); make that first call before any stream capture.  Every call on a
+ * device shares the one scratch array, so calls whose work overlaps on the GPU race: keep them on one
+ * stream, or order them.  d_err is cleared by the call itself. */
+#define ZC_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
+int zc_decompress_noalloc(const uint8_t *d_comp, const uint64_t *d_comp_offs, const uint32_t *d_comp_lens,
+                          const uint8_t *d_methods, const uint32_t *d_raw_lens, uint32_t nb, uint32_t block_log,
+                          uint8_t *d_out, const uint64_t *d_out_offs, uint32_t *d_crcs, uint32_t *d_err, void *stream);
+
 /* CRC-32 of host bytes on the GPU (crc32::of, src/crc32.h:51), and CRC combination on the host
  * (crc32::combine, src/crc32.h:60-66): the CRC of A followed by B. */
 int zc_crc32(zc_ctx *ctx, const uint8_t *data, size_t n, uint32_t *crc);
