@@ -218,17 +218,24 @@ def run_ours(args):
     sh = stream.cuda_stream
     chunks = [(b0, min(per, nb - b0)) for b0 in range(0, nb, per)]
 
+    chunk_base = torch.tensor([b0 * B for b0, k in chunks for _ in range(k)], dtype=torch.int64, device=dev)
+    goffs = torch.zeros(nb, dtype=torch.int64, device=dev)
+    dec_per = codec.batch_bytes_decode(bl) // B  # blocks per decoder launch
+
     def compress():
+        # one launch per stage per chunk of blocks; each chunk's record bodies land in its own slice of d_out
         for ci, (b0, k) in enumerate(chunks):
             o = b0 * B
             codec.compress_device(d_in, offs[b0:], lens[b0:], k, bl, methods[b0:], clens[b0:], crcs[b0:],
                                   d_out[o:o + k * B + 64], ooffs[b0:], totals[ci:], stream=sh)
+        with torch.cuda.stream(stream):
+            torch.add(ooffs, chunk_base, out=goffs)  # record offsets from the start of d_out
 
     def decompress():
-        for ci, (b0, k) in enumerate(chunks):
-            o = b0 * B
-            codec.decompress_device(d_out[o:o + k * B + 64], ooffs[b0:], clens[b0:], methods[b0:], lens[b0:], k, bl,
-                                    d_dec, offs[b0:], dcrcs[b0:], errs[b0:], stream=sh)
+        for b0 in range(0, nb, dec_per):
+            k = min(dec_per, nb - b0)
+            codec.decompress_device(d_out, goffs[b0:], clens[b0:], methods[b0:], lens[b0:], k, bl, d_dec, offs[b0:],
+                                    dcrcs[b0:], errs[b0:], stream=sh)
 
     def barrier():
         if ws > 1:

@@ -148,9 +148,51 @@ __global__ void __launch_bounds__(64) k_dec_streams(DecArgs A) {
 }
 
 // ---------------------------------------------------------------- LZ replay
-// copies n bytes; no ordering between the bytes is needed (source and destination do not overlap)
-__device__ __forceinline__ void lane_copy(uint8_t* d, const uint8_t* s, uint32_t n) {
-  for (uint32_t i = 0; i < n; ++i) d[i] = s[i];
+// A chunk of at most 32 tokens of one group, as the warp's shared table: output start, match start,
+// offset and literal start of each token (start[c] = the chunk's end).
+struct ChunkTable {
+  uint32_t start[33], ms[32], dist[32], lik[32];
+};
+
+// the byte at output position q of token k: its own literal, or a match byte, whose source is output
+// from before the group or this token's own literals (src/codec2.h:1-6); an overlapping match (D < M)
+// repeats the D bytes before it, so the source of match byte i is ms - D + (i mod D)
+__device__ __forceinline__ uint32_t chunk_byte(const ChunkTable& T, const uint8_t* o, const uint8_t* lit, uint32_t q,
+                                               uint32_t k) {
+  const uint32_t opk = T.start[k], ms = T.ms[k];
+  if (q < ms) return lit[T.lik[k] + (q - opk)];
+  const uint32_t D = T.dist[k];
+  uint32_t s = q - D;
+  if (s >= ms) s = ms - D + (q - ms) % D;
+  return s >= opk ? lit[T.lik[k] + (s - opk)] : o[s];
+}
+
+// all lanes fill the chunk's output [op, op_end): 4 bytes each per round, whole aligned words stored as
+// words.  No byte of a group depends on another byte of the same group, so the order is free.
+__device__ __forceinline__ void fill_chunk(const ChunkTable& T, uint8_t* o, const uint8_t* lit, uint32_t c,
+                                          uint32_t op, uint32_t op_end) {
+  const uintptr_t ob = (uintptr_t)o;
+  const int64_t qa = (int64_t)(((ob + op) & ~(uintptr_t)3) - ob);
+  for (int64_t q0 = qa + 4 * (int64_t)lane_id(); q0 < (int64_t)op_end; q0 += 128) {
+    const uint32_t qs = (uint32_t)(q0 > (int64_t)op ? q0 : (int64_t)op);
+    uint32_t lo = 0, hi = c;  // start[lo] <= qs < start[hi]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (T.start[mid] <= qs) lo = mid; else hi = mid;
+    }
+    uint32_t k = lo, w = 0;
+    const bool full = q0 >= (int64_t)op && q0 + 4 <= (int64_t)op_end;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t q = q0 + j;
+      if (q < (int64_t)op || q >= (int64_t)op_end) continue;
+      while ((uint32_t)q >= T.start[k + 1]) ++k;
+      const uint32_t v = chunk_byte(T, o, lit, (uint32_t)q, k);
+      if (full) w |= v << (8 * j);
+      else o[q] = (uint8_t)v;
+    }
+    if (full) *reinterpret_cast<uint32_t*>(o + q0) = w;
+  }
 }
 // a warp copies n bytes, coalesced (src and dst do not overlap)
 __device__ inline void warp_copy(uint8_t* d, const uint8_t* s, uint32_t n) {
@@ -168,8 +210,10 @@ __device__ inline void warp_copy(uint8_t* d, const uint8_t* s, uint32_t n) {
 }
 
 __global__ void __launch_bounds__(128) k_dec_lz(DecArgs A) {
+  __shared__ ChunkTable tables[4];
   const uint32_t b = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (b >= A.nb) return;
+  ChunkTable& T = tables[threadIdx.x >> 5];
   const uint32_t lane = lane_id();
   const uint32_t raw = A.raw_len[b], method = A.method[b], clen = A.comp_len[b], B = A.B;
   uint8_t* o = A.out + A.out_off[b];
@@ -237,15 +281,13 @@ __global__ void __launch_bounds__(128) k_dec_lz(DecArgs A) {
       const uint32_t ms = opk + L;
       if (on && ((uint64_t)lik + L > m.nl || (uint64_t)opk + tot > raw || D == 0 || D > ms)) bad = true;
       if (__any_sync(kFull, bad)) { if (lane == 0) set_err(A.err, b, E_TOKEN); return; }
-      if (on) {
-        lane_copy(o + opk, lit + lik, L);
-        // the source is output from before the group, or this token's own literals / output
-        const uint8_t* src = o + ms - D;
-        uint8_t* dst = o + ms;
-        if (D >= M) lane_copy(dst, src, M);
-        else for (uint32_t i = 0; i < M; ++i) dst[i] = src[i];
-      }
-      op += __shfl_sync(kFull, oincl, 31);
+      const uint32_t op_end = op + __shfl_sync(kFull, oincl, 31);
+      if (on) { T.start[lane] = opk; T.ms[lane] = ms; T.dist[lane] = D; T.lik[lane] = lik; }
+      if (lane == 0) T.start[c] = op_end;
+      __syncwarp();
+      fill_chunk(T, o, lit, c, op, op_end);
+      __syncwarp();
+      op = op_end;
       li += __shfl_sync(kFull, lincl, 31);
       ei += __shfl_sync(kFull, xincl, 31);
       bp += __shfl_sync(kFull, bincl, 31);

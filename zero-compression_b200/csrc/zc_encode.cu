@@ -23,10 +23,13 @@
 
 namespace zc {
 
-// per-position match record: NONE, SAT (longest candidate reached cmp_cap: finish on demand), or the
-// exact (length - 4) << 20 | (distance - 1); lengths are <= 4096, so the top 12 bits never read 0xFFF
+// per-position match record: NONE; SAT | k (a candidate reached cmp_cap, the first of them k steps back
+// in the chain: finished on demand by the parse); or the exact (length - 4) << 20 | (distance - 1).
+// Lengths are <= 4096, so an exact record never has 0xFFF in its top 12 bits.
 constexpr uint32_t M_NONE = 0xFFFFFFFFu;
 constexpr uint32_t M_SAT = 0xFFF00000u;
+__device__ __forceinline__ bool m_is_sat(uint32_t v) { return (v >> 20) == 0xFFFu && v != M_NONE; }
+constexpr uint32_t kWin = 32;  // bytes of each sorted position kept in shared memory by the match pass
 __device__ __forceinline__ uint32_t m_pack(uint32_t m, uint32_t d) { return ((m - 4u) << 20) | (d - 1u); }
 __device__ __forceinline__ uint32_t m_len(uint32_t v) { return (v >> 20) + 4u; }
 __device__ __forceinline__ uint32_t m_dist(uint32_t v) { return (v & 0xFFFFFu) + 1u; }
@@ -56,105 +59,194 @@ __device__ __forceinline__ uint32_t lcp(const uint8_t* base, uint64_t a, uint64_
 }
 
 // ---------------------------------------------------------------- 1. stable sort by hash
+// Two stable LSD passes over the 16-bit hash (low byte, then high byte).  Each pass walks the block in
+// tiles of 4096 positions: a tile is ranked per digit (per-warp counts, __match_any_sync ranks), reordered
+// by digit in shared memory, and written out so that each digit's run is one contiguous global write.
+// Both passes' digit histograms come from one sweep.  Dynamic shared memory: kSortSmem bytes.
+constexpr uint32_t kSortTile = 4096, kSortPer = kSortTile / 1024;  // positions per tile, per thread
+constexpr size_t kSortSmem = 32 * 256 * 4 + kSortTile * 6 + 5 * 256 * 4;
+
 __global__ void __launch_bounds__(1024) k_enc_sort(EncArgs A) {
+  extern __shared__ uint32_t ss[];
+  uint32_t (*cw)[256] = reinterpret_cast<uint32_t (*)[256]>(ss);  // per-warp digit counts of a tile
+  uint32_t* st_pos = ss + 32 * 256;                                // the tile reordered by digit
+  uint16_t* st_h = reinterpret_cast<uint16_t*>(st_pos + kSortTile);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(st_h + kSortTile);  // [2][256] block histograms
+  uint32_t* base = hist + 512;                                     // digit start in the block
+  uint32_t* tds = base + 256;                                      // digit start in the tile
+  uint32_t* tot = tds + 256;                                       // digit count in the tile
   const uint32_t b = blockIdx.x;
   const uint32_t n = A.in_len[b];
   const uint32_t count = n >= 4 ? n - 3 : 0;  // positions with 4 bytes left (src/codec2.h:52, 58)
   if (!count) return;
-  __shared__ uint32_t hist[32][256];
-  __shared__ uint32_t tot[256];
   const uint32_t tid = threadIdx.x, w = tid >> 5, lane = tid & 31u;
-  const uint32_t cw = (count + 31) / 32;
-  const uint32_t beg = min(w * cw, count), end = min(beg + cw, count);
-  const uint64_t base = A.in_off[b];
+  const uint64_t in0 = A.in_off[b];
   const size_t so = (size_t)b * A.B;
   uint32_t* tpos = A.tmp_pos + so;
   uint16_t* th = A.tmp_h + so;
   uint32_t* spos = A.srt_pos + so;
   uint16_t* sh = A.srt_h + so;
+  for (uint32_t i = tid; i < 512; i += 1024) hist[i] = 0;
+  __syncthreads();
+  for (uint32_t i = tid; i < count; i += 1024) {
+    const uint32_t h = hash16(A.in, in0 + i);
+    atomicAdd(&hist[h & 0xFFu], 1u);
+    atomicAdd(&hist[256 + (h >> 8)], 1u);
+  }
+  __syncthreads();
   for (int pass = 0; pass < 2; ++pass) {
-    for (uint32_t i = tid; i < 32 * 256; i += blockDim.x) (&hist[0][0])[i] = 0;
-    __syncthreads();
-    for (uint32_t i = beg + lane; i < end; i += 32) {
-      const uint32_t h = pass == 0 ? hash16(A.in, base + i) : th[i];
-      atomicAdd(&hist[w][pass == 0 ? (h & 0xFFu) : (h >> 8)], 1u);
-    }
-    __syncthreads();
-    if (tid < 256) {
-      uint32_t run = 0;
-      for (uint32_t k = 0; k < 32; ++k) { const uint32_t c = hist[k][tid]; hist[k][tid] = run; run += c; }
-      tot[tid] = run;
-    }
-    __syncthreads();
-    if (w == 0) {
-      uint32_t v[8], s = 0;
+    if (w == 0) {  // digit starts: exclusive scan of this pass's histogram
+      uint32_t v[8], sum = 0;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) { v[k] = tot[lane * 8 + k]; s += v[k]; }
-      uint32_t ex = warp_incl_scan(s) - s;
+      for (int k = 0; k < 8; ++k) { v[k] = hist[pass * 256 + lane * 8 + k]; sum += v[k]; }
+      uint32_t ex = warp_incl_scan(sum) - sum;
 #pragma unroll
-      for (int k = 0; k < 8; ++k) { tot[lane * 8 + k] = ex; ex += v[k]; }
+      for (int k = 0; k < 8; ++k) { base[lane * 8 + k] = ex; ex += v[k]; }
     }
-    __syncthreads();
-    if (tid < 256)
-      for (uint32_t k = 0; k < 32; ++k) hist[k][tid] += tot[tid];
-    __syncthreads();
-    for (uint32_t i0 = beg; i0 < end; i0 += 32) {
-      const uint32_t i = i0 + lane;
-      const bool on = i < end;
-      uint32_t h = 0, p = 0;
-      if (on) {
-        if (pass == 0) { p = i; h = hash16(A.in, base + i); }
-        else { p = tpos[i]; h = th[i]; }
+    for (uint32_t t0 = 0; t0 < count; t0 += kSortTile) {
+      for (uint32_t i = tid; i < 32 * 256; i += 1024) (&cw[0][0])[i] = 0;
+      __syncthreads();
+      // rank: warp w holds tile elements [128 w, 128 w + 128), 32 per round, in order
+      uint32_t kp[kSortPer], kh[kSortPer], kr[kSortPer];
+#pragma unroll
+      for (uint32_t j = 0; j < kSortPer; ++j) {
+        const uint32_t i = t0 + w * (32 * kSortPer) + j * 32 + lane;
+        const bool on = i < count;
+        uint32_t p = 0, h = 0;
+        if (on) {
+          if (pass == 0) { p = i; h = hash16(A.in, in0 + i); }
+          else { p = tpos[i]; h = th[i]; }
+        }
+        const uint32_t d = pass == 0 ? (h & 0xFFu) : (h >> 8);
+        const unsigned act = __ballot_sync(kFull, on);
+        uint32_t rk = 0;
+        if (on) {
+          const unsigned peers = __match_any_sync(act, d);
+          const uint32_t c = cw[w][d];
+          rk = c + __popc(peers & ((1u << lane) - 1u));
+          __syncwarp(act);
+          if ((peers & ((1u << lane) - 1u)) == 0) cw[w][d] = c + __popc(peers);
+        }
+        __syncwarp();
+        kp[j] = p; kh[j] = h; kr[j] = on ? rk : 0xFFFFFFFFu;
       }
-      const uint32_t d = pass == 0 ? (h & 0xFFu) : (h >> 8);
-      const unsigned act = __ballot_sync(kFull, on);
-      if (on) {
-        const unsigned peers = __match_any_sync(act, d);
-        const uint32_t rk = __popc(peers & ((1u << lane) - 1u));
-        const uint32_t dest = hist[w][d] + rk;
-        if (pass == 0) { tpos[dest] = p; th[dest] = (uint16_t)h; }
-        else { spos[dest] = p; sh[dest] = (uint16_t)h; }
-        __syncwarp(act);
-        if (rk == 0) hist[w][d] += __popc(peers);
+      __syncthreads();
+      if (tid < 256) {  // per digit: counts of the warps before, the tile's count
+        uint32_t run = 0;
+        for (uint32_t k = 0; k < 32; ++k) { const uint32_t c = cw[k][tid]; cw[k][tid] = run; run += c; }
+        tot[tid] = run;
       }
-      __syncwarp();
+      __syncthreads();
+      if (w == 0) {
+        uint32_t v[8], sum = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) { v[k] = tot[lane * 8 + k]; sum += v[k]; }
+        uint32_t ex = warp_incl_scan(sum) - sum;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) { tds[lane * 8 + k] = ex; ex += v[k]; }
+      }
+      __syncthreads();
+#pragma unroll
+      for (uint32_t j = 0; j < kSortPer; ++j) {
+        if (kr[j] == 0xFFFFFFFFu) continue;
+        const uint32_t d = pass == 0 ? (kh[j] & 0xFFu) : (kh[j] >> 8);
+        const uint32_t at = tds[d] + cw[w][d] + kr[j];
+        st_pos[at] = kp[j];
+        st_h[at] = (uint16_t)kh[j];
+      }
+      __syncthreads();
+      const uint32_t tn = min(kSortTile, count - t0);
+      for (uint32_t i = tid; i < tn; i += 1024) {
+        const uint32_t h = st_h[i];
+        const uint32_t d = pass == 0 ? (h & 0xFFu) : (h >> 8);
+        const uint32_t dest = base[d] + (i - tds[d]);
+        if (pass == 0) { tpos[dest] = st_pos[i]; th[dest] = (uint16_t)h; }
+        else { spos[dest] = st_pos[i]; sh[dest] = (uint16_t)h; }
+      }
+      __syncthreads();
+      if (tid < 256) base[tid] += tot[tid];
+      __syncthreads();
     }
     __syncthreads();
   }
 }
 
 // ---------------------------------------------------------------- 2. capped matches at every position
+// the first differing byte of two 32-byte windows (32 when equal)
+__device__ __forceinline__ uint32_t lcp32(const uint4& a0, const uint4& a1, const uint4& b0, const uint4& b1) {
+  uint32_t x;
+  if ((x = a0.x ^ b0.x)) return ((uint32_t)__ffs(x) - 1u) >> 3;
+  if ((x = a0.y ^ b0.y)) return 4 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  if ((x = a0.z ^ b0.z)) return 8 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  if ((x = a0.w ^ b0.w)) return 12 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  if ((x = a1.x ^ b1.x)) return 16 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  if ((x = a1.y ^ b1.y)) return 20 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  if ((x = a1.z ^ b1.z)) return 24 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  if ((x = a1.w ^ b1.w)) return 28 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  return 32;
+}
+
+// One CTA per 256 consecutive sorted positions of a block.  The entries it needs (its own and the
+// `depth` before them) are staged once in shared memory with the first 32 bytes at each position, so
+// a candidate costs a few shared loads and XORs instead of random global reads.  Dynamic shared memory:
+// (256 + depth) * (32 + 4 + 2) bytes.
 __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
-  const uint32_t b = blockIdx.y;
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  extern __shared__ uint4 sm[];
+  const uint32_t b = blockIdx.y, t = threadIdx.x;
+  const uint32_t r0 = blockIdx.x * 256;
   const uint32_t n = A.in_len[b];
+  if (r0 >= n) return;
   const uint32_t count = n >= 4 ? n - 3 : 0;
   const size_t so = (size_t)b * A.B;
-  if (r >= count) { if (r < n) A.minfo[so + r] = M_NONE; return; }
-  const uint32_t* spos = A.srt_pos + so;
-  const uint16_t* sh = A.srt_h + so;
-  const uint32_t p = spos[r], h = sh[r];
-  A.rank[so + p] = r;
+  const uint32_t D = (uint32_t)A.depth;
+  const uint32_t cap_e = 256 + D;
+  uint4* wlo = sm;
+  uint4* whi = wlo + cap_e;
+  uint32_t* spos = reinterpret_cast<uint32_t*>(whi + cap_e);
+  uint16_t* sh = reinterpret_cast<uint16_t*>(spos + cap_e);
+  const uint32_t e0 = r0 > D ? r0 - D : 0, e1 = min(r0 + 256, count);
   const uint64_t base = A.in_off[b];
-  const uint32_t lim = min(kMaxMatch, n - p), cap = min(A.cmp_cap, lim);
-  const uint64_t ap = base + p;
-  uint32_t best = 0, bd = 0;
-  const uint32_t kmax = min((uint32_t)A.depth, r);
+  const uint32_t* w32 = reinterpret_cast<const uint32_t*>(A.in);
+  const uint64_t wend = (base + n + 3) >> 2;  // words at or past it are not read (they lie past the block)
+  for (uint32_t i = t; e0 + i < e1; i += 256) {
+    const uint32_t r = e0 + i;
+    const uint32_t p = A.srt_pos[so + r];
+    spos[i] = p;
+    sh[i] = A.srt_h[so + r];
+    const uint64_t a = base + p, wa = a >> 2;
+    const uint32_t shf = (uint32_t)(a & 3u) * 8u;
+    uint32_t w[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) w[q] = wa + q < wend ? __ldg(w32 + wa + q) : 0u;
+    uint32_t v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = __funnelshift_r(w[q], w[q + 1], shf);
+    wlo[i] = make_uint4(v[0], v[1], v[2], v[3]);
+    whi[i] = make_uint4(v[4], v[5], v[6], v[7]);
+  }
+  __syncthreads();
+  const uint32_t r = r0 + t;
+  if (r >= count) { if (r < n) A.minfo[so + r] = M_NONE; return; }
+  const uint32_t li = r - e0;
+  const uint32_t p = spos[li], h = sh[li];
+  A.rank[so + p] = r;
+  const uint32_t lim = min(kMaxMatch, n - p), cap = min(min(A.cmp_cap, kWin), lim);
+  const uint4 p0 = wlo[li], p1 = whi[li];
+  uint32_t best = 0, bd = 0, kf = 0;
+  const uint32_t kmax = min(D, r);
   for (uint32_t k = 1; k <= kmax; ++k) {
-    if (sh[r - k] != h) break;
-    const uint32_t j = spos[r - k];
-    const uint64_t aj = base + j;
-    if (best && __ldg(A.in + aj + best) != __ldg(A.in + ap + best)) continue;
-    const uint32_t l = lcp(A.in, aj, ap, cap);
+    const uint32_t e = li - k;
+    if (sh[e] != h) break;
+    const uint32_t l = min(lcp32(wlo[e], whi[e], p0, p1), cap);
     if (l > best) {
       best = l;
-      bd = p - j;
-      if (best == cap) break;
+      bd = p - spos[e];
+      if (best == cap) { kf = k; break; }
     }
   }
   uint32_t v;
   if (best < 4) v = M_NONE;
-  else if (best == cap && cap < lim) v = M_SAT;
+  else if (best == cap && cap < lim) v = M_SAT | kf;
   else v = m_pack(best, bd);
   A.minfo[so + p] = v;
 }
@@ -173,13 +265,14 @@ struct ParseBlock {
 // the exact match at p (finishing a capped one: the whole chain compared up to 4096 bytes)
 __device__ uint32_t exact_match(const ParseBlock& P, uint32_t p) {
   const uint32_t v = P.minfo[p];
-  if (v != M_SAT) return v;
+  if (!m_is_sat(v)) return v;
   const uint32_t r = P.rank[p], h = P.sh[r];
   const uint32_t lim = min(kMaxMatch, P.n - p);
   const uint64_t ap = P.base + p;
   uint32_t best = 0, bd = 0;
   const uint32_t kmax = min(P.depth, r);
-  for (uint32_t k = 1; k <= kmax; ++k) {
+  // candidates before the first that reached the cap are shorter than it: start there
+  for (uint32_t k = max(1u, v & 0xFFFFFu); k <= kmax; ++k) {
     if (P.sh[r - k] != h) break;
     const uint32_t j = P.spos[r - k];
     const uint64_t aj = P.base + j;
@@ -643,10 +736,18 @@ void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Sta
   if (!A.nb) return;
   launch_crc(crc_in, st, S, "k_crc_in");
   S.begin("k_enc_sort", st);
-  k_enc_sort<<<A.nb, 1024, 0, st>>>(A);
+  static unsigned long long sort_smem_set = 0;  // devices that allow the sort its shared memory
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(sort_smem_set >> dev & 1ull)) {
+    cudaFuncSetAttribute(k_enc_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmem);
+    sort_smem_set |= 1ull << dev;
+  }
+  k_enc_sort<<<A.nb, 1024, kSortSmem, st>>>(A);
   S.end(st);
   S.begin("k_enc_match", st);
-  k_enc_match<<<dim3((A.B + 255) / 256, A.nb), 256, 0, st>>>(A);
+  const size_t msm = (size_t)(256 + A.depth) * (2 * sizeof(uint4) + 4 + 2);
+  k_enc_match<<<dim3((A.B + 255) / 256, A.nb), 256, msm, st>>>(A);
   S.end(st);
   S.begin("k_enc_parse", st);
   k_enc_parse<<<A.nb, 256, 0, st>>>(A);
