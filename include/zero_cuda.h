@@ -88,8 +88,9 @@ int zc_decompress(zc_ctx *ctx, const uint8_t *comp, const uint64_t *comp_offs, c
 /* ---- device-resident forms: every pointer is device memory, work is queued on `stream` (a
  * cudaStream_t; NULL for the legacy default stream) and the call returns once it is queued.  For
  * callers that keep data on the GPU, and for measuring the kernels without host copies.
- * d_in must be 4-byte aligned with at least 16 readable bytes after the last block (the match finder
- * reads whole aligned words, as the reference's kernels do: kernels/zero.cl:30-31).
+ * d_in must be 16-byte aligned with at least 64 readable bytes after the last block (the match finder
+ * reads whole aligned words and 16-byte groups, as the reference's kernels read words past a block:
+ * kernels/zero.cl:30-31).
  *
  * zc_compress_device: nb blocks at d_in + d_in_offs[b], d_in_lens[b] bytes each.  Writes d_methods,
  * d_comp_lens, d_crcs (may be NULL) and the payloads packed into d_out (out_cap bytes) at d_out_offs[b];

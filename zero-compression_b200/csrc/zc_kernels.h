@@ -54,7 +54,7 @@ void launch_crc(const CrcArgs& A, cudaStream_t st, Stages& S, const char* name);
 
 // ---- encoder
 struct EncArgs {
-  const uint8_t* in;          // block b: in_len[b] bytes at in + in_off[b]; >= 16 readable bytes after the last
+  const uint8_t* in;          // block b: in_len[b] bytes at in + in_off[b]; 16-aligned, >= 64 readable bytes after the last
   const uint64_t* in_off;
   const uint32_t* in_len;
   uint32_t nb, B, block_log;
