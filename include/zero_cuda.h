@@ -126,6 +126,14 @@ int zc_decompress_noalloc(const uint8_t *d_comp, const uint64_t *d_comp_offs, co
                           const uint8_t *d_methods, const uint32_t *d_raw_lens, uint32_t nb, uint32_t block_log,
                           uint8_t *d_out, const uint64_t *d_out_offs, uint32_t *d_crcs, uint32_t *d_err, void *stream);
 
+/* CUDA graphs for the device-resident forms (no reference counterpart: the reference's Level Zero command
+ * list replays nothing).  With on != 0, the first zc_compress_device / zc_decompress_device call with a
+ * given set of arguments and a non-NULL stream captures its launches into a graph; later calls with the
+ * same arguments replay it (one launch).  A batch of fixed capacity padded with zero-length blocks keeps
+ * its arguments, so one graph serves every batch.  Graphs are dropped when the context's scratch grows
+ * and when turned off. */
+int zc_set_graphs(zc_ctx *ctx, int on);
+
 /* CRC-32 of host bytes on the GPU (crc32::of, src/crc32.h:51), and CRC combination on the host
  * (crc32::combine, src/crc32.h:60-66): the CRC of A followed by B. */
 int zc_crc32(zc_ctx *ctx, const uint8_t *data, size_t n, uint32_t *crc);

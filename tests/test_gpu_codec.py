@@ -189,3 +189,38 @@ def test_reference_api_shapes(codec):
     assert codec.decompress(ins) == data
     assert codec.batch_bytes(18) >= B and codec.batch_bytes_decode(18) >= B
     assert "GPU" in codec.name()
+
+
+def test_graph_replay_matches_direct(codec):
+    """Device-resident calls captured as CUDA graphs and replayed give the same bytes as direct launches."""
+    import torch
+    import datagen as G
+    dev = torch.device("cuda", 0)
+    bl, B = 16, 1 << 16
+    data = np.concatenate([G.text_mix(200000, 61), G.random_bytes(70000, 62), G.lz_mix(150000, 16, 63)])
+    n, nb = data.size, (data.size + B - 1) // B
+    d_in = torch.zeros(n + 64, dtype=torch.uint8, device=dev)
+    d_in[:n] = torch.from_numpy(data).to(dev)
+    offs = torch.arange(nb, dtype=torch.int64, device=dev) * B
+    lens = torch.clamp(n - offs, max=B).to(torch.int32)
+    stream = torch.cuda.Stream(device=dev)
+    res = []
+    for graphs in (False, True, True):
+        codec.set_graphs(graphs)
+        outs = dict(m=torch.zeros(nb, dtype=torch.uint8, device=dev), l=torch.zeros(nb, dtype=torch.int32, device=dev),
+                    c=torch.zeros(nb, dtype=torch.int32, device=dev), o=torch.zeros(n + 64, dtype=torch.uint8, device=dev),
+                    f=torch.zeros(nb, dtype=torch.int64, device=dev), t=torch.zeros(1, dtype=torch.int64, device=dev),
+                    d=torch.zeros(n + 64, dtype=torch.uint8, device=dev), dc=torch.zeros(nb, dtype=torch.int32, device=dev),
+                    e=torch.zeros(nb, dtype=torch.int32, device=dev))
+        for _ in range(2):  # (a second call replays the captured graph)
+            codec.compress_device(d_in, offs, lens, nb, bl, outs["m"], outs["l"], outs["c"], outs["o"], outs["f"],
+                                  outs["t"], stream=stream.cuda_stream)
+            codec.decompress_device(outs["o"], outs["f"], outs["l"], outs["m"], lens, nb, bl, outs["d"], offs,
+                                    outs["dc"], outs["e"], stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        assert torch.equal(outs["d"][:n], d_in[:n]) and not outs["e"].any()
+        tot = int(outs["t"].item())
+        res.append((outs["m"].cpu(), outs["l"].cpu(), outs["c"].cpu(), outs["o"][:tot].cpu()))
+    codec.set_graphs(False)
+    for r in res[1:]:
+        assert all(torch.equal(a, b) for a, b in zip(res[0], r))

@@ -102,8 +102,18 @@ void zc::Stages::end(cudaStream_t st) {
   R->pending.push_back({R->open_name, R->open_ev, e});
 }
 
+// a captured launch sequence, replayed when a device entry point is called again with the same arguments
+struct GraphEntry {
+  int kind;
+  uint64_t key[24];
+  cudaGraphExec_t exec;
+  uint64_t launches;  // kernels in the graph
+};
+
 struct zc_ctx {
   int device = 0;
+  bool graphs = false;
+  std::vector<GraphEntry> graph_cache;
   cudaStream_t stream = nullptr;
   std::string err, name;
   uint32_t block_log = 18;
@@ -164,8 +174,14 @@ void release(DevBuf& b) {
   b.n = 0;
 }
 
+void drop_graphs(zc_ctx* c) {
+  for (GraphEntry& g : c->graph_cache) cudaGraphExecDestroy(g.exec);
+  c->graph_cache.clear();
+}
+
 int ensure_enc(zc_ctx* c, uint32_t nb, uint32_t block_log) {
   if (nb <= c->enc_nb && block_log == c->enc_bl) return ZC_OK;
+  drop_graphs(c);  // (captured graphs name the scratch being replaced)
   const size_t B = (size_t)1 << block_log, TC = zc::tok_cap((uint32_t)B), EC = zc::ext_cap((uint32_t)B);
   const size_t N = (size_t)nb * B;
   ZC_CUDA(grow(c->e_tmp_pos, N * 4));
@@ -196,6 +212,7 @@ int ensure_enc(zc_ctx* c, uint32_t nb, uint32_t block_log) {
 
 int ensure_dec(zc_ctx* c, uint32_t nb, uint32_t block_log) {
   if (nb <= c->dec_nb && block_log == c->dec_bl) return ZC_OK;
+  drop_graphs(c);
   const size_t B = (size_t)1 << block_log, TC = zc::tok_cap((uint32_t)B), EC = zc::ext_cap((uint32_t)B);
   ZC_CUDA(grow(c->d_lit, (size_t)nb * B));
   ZC_CUDA(grow(c->d_tok, (size_t)nb * TC));
@@ -272,6 +289,41 @@ int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs,
     zc::launch_crc(C, st, c->stages, "k_crc_out");
   }
   return check_launch(c, "decoder launch");
+}
+
+// Runs `body` on stream st, through a CUDA graph when graphs are on: the first call with a given key
+// captures the launches, later calls replay them.  Scratch must already be sized (a capture allocates
+// nothing) and per-stage timing is off inside captures.
+template <class F>
+int with_graph(zc_ctx* c, int kind, const uint64_t* key, int nkey, cudaStream_t st, F body) {
+  if (!c->graphs || st == nullptr) return body();
+  for (GraphEntry& g : c->graph_cache) {
+    if (g.kind != kind || memcmp(g.key, key, sizeof(uint64_t) * nkey) != 0) continue;
+    ZC_CUDA(cudaGraphLaunch(g.exec, st));
+    c->stages.launches += g.launches;
+    return ZC_OK;
+  }
+  const bool timing = c->stages.timing;
+  c->stages.timing = false;
+  const uint64_t l0 = c->stages.launches;
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) { c->stages.timing = timing; return cuda_fail(c, e, "cudaStreamBeginCapture"); }
+  int r = body();
+  e = cudaStreamEndCapture(st, &graph);
+  c->stages.timing = timing;
+  if (r) { if (graph) cudaGraphDestroy(graph); return r; }
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+  GraphEntry g{};
+  g.kind = kind;
+  memcpy(g.key, key, sizeof(uint64_t) * nkey);
+  g.launches = c->stages.launches - l0;
+  e = cudaGraphInstantiate(&g.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+  c->graph_cache.push_back(g);
+  ZC_CUDA(cudaGraphLaunch(g.exec, st));
+  return ZC_OK;
 }
 
 // host-pointer compress of nb blocks whose bytes lie in host memory [lo, lo + span)
@@ -371,6 +423,7 @@ int zc_open(zc_ctx** out, int device) {
     return ZC_E_DEVICE;
   }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = zc::prepare_kernels();
   if (e == cudaSuccess) e = cudaMalloc(&c->d_crct, sizeof(zc::CrcTables));
   if (e == cudaSuccess) {
     zc::CrcTables T;
@@ -389,6 +442,7 @@ void zc_close(zc_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
   for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_rank, &c->e_minfo, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
                     &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
                     &c->e_bits, &c->e_lanes, &c->e_freq, &c->e_lanelen, &c->e_sinfo, &c->e_slab, &c->d_lit, &c->d_tok,
@@ -471,8 +525,17 @@ int zc_compress_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_in_offs
                        void* stream) {
   if (!c) return ZC_E_ARG;
   ZC_CUDA(cudaSetDevice(c->device));
-  return encode_device(c, d_in, d_in_offs, d_in_lens, nb, block_log, level, d_methods, d_comp_lens, d_crcs, d_out,
-                       out_cap, d_out_offs, d_total, 1, static_cast<cudaStream_t>(stream));
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  if (nb > enc_blocks_per_launch(block_log)) return fail(c, ZC_E_ARG, "too many blocks for one launch");
+  if (int r = ensure_enc(c, nb, block_log)) return r;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const uint64_t key[] = {(uint64_t)d_in, (uint64_t)d_in_offs, (uint64_t)d_in_lens, nb, block_log, (uint64_t)level,
+                          (uint64_t)d_methods, (uint64_t)d_comp_lens, (uint64_t)d_crcs, (uint64_t)d_out, out_cap,
+                          (uint64_t)d_out_offs, (uint64_t)d_total, (uint64_t)st};
+  return with_graph(c, 0, key, (int)(sizeof key / sizeof key[0]), st, [&] {
+    return encode_device(c, d_in, d_in_offs, d_in_lens, nb, block_log, level, d_methods, d_comp_lens, d_crcs, d_out,
+                         out_cap, d_out_offs, d_total, 1, st);
+  });
 }
 
 int zc_decompress_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs, const uint32_t* d_comp_lens,
@@ -481,8 +544,24 @@ int zc_decompress_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_com
   if (!c) return ZC_E_ARG;
   ZC_CUDA(cudaSetDevice(c->device));
   if (nb > dec_blocks_per_launch(block_log)) return fail(c, ZC_E_ARG, "too many blocks for one launch");
-  return decode_device(c, d_comp, d_comp_offs, d_comp_lens, d_methods, d_raw_lens, nb, block_log, d_out, d_out_offs,
-                       d_crcs, d_err, static_cast<cudaStream_t>(stream));
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  if (int r = ensure_dec(c, std::max(nb, 1u), block_log)) return r;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const uint64_t key[] = {(uint64_t)d_comp, (uint64_t)d_comp_offs, (uint64_t)d_comp_lens, (uint64_t)d_methods,
+                          (uint64_t)d_raw_lens, nb, block_log, (uint64_t)d_out, (uint64_t)d_out_offs, (uint64_t)d_crcs,
+                          (uint64_t)d_err, (uint64_t)st};
+  return with_graph(c, 1, key, (int)(sizeof key / sizeof key[0]), st, [&] {
+    return decode_device(c, d_comp, d_comp_offs, d_comp_lens, d_methods, d_raw_lens, nb, block_log, d_out, d_out_offs,
+                         d_crcs, d_err, st);
+  });
+}
+
+int zc_set_graphs(zc_ctx* c, int on) {
+  if (!c) return ZC_E_ARG;
+  ZC_CUDA(cudaSetDevice(c->device));
+  if (!on) drop_graphs(c);
+  c->graphs = on != 0;
+  return ZC_OK;
 }
 
 int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, const uint32_t* comp_lens,

@@ -732,17 +732,14 @@ __global__ void __launch_bounds__(256) k_enc_emit(EncArgs A) {
   for (uint32_t k = i + threadIdx.x; k < len; k += blockDim.x) d[k] = s[k];
 }
 
+cudaError_t prepare_kernels() {  // with the device current, once per context
+  return cudaFuncSetAttribute(k_enc_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmem);
+}
+
 void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Stages& S) {
   if (!A.nb) return;
   launch_crc(crc_in, st, S, "k_crc_in");
   S.begin("k_enc_sort", st);
-  static unsigned long long sort_smem_set = 0;  // devices that allow the sort its shared memory
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !(sort_smem_set >> dev & 1ull)) {
-    cudaFuncSetAttribute(k_enc_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmem);
-    sort_smem_set |= 1ull << dev;
-  }
   k_enc_sort<<<A.nb, 1024, kSortSmem, st>>>(A);
   S.end(st);
   S.begin("k_enc_match", st);

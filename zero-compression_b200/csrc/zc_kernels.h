@@ -98,5 +98,6 @@ __host__ __device__ inline uint64_t lanes_per_block(uint32_t B) { return lane_ba
 __host__ __device__ inline uint32_t bits_cap(uint32_t B) { return 5 * B / 8 + 64; }
 
 void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Stages& S);
+cudaError_t prepare_kernels();  // per-kernel attributes (the sort's shared memory), the device current
 
 }  // namespace zc

@@ -86,6 +86,7 @@ def lib():
         L.zc_launch_count.argtypes = [_vp]
         L.zc_launch_count.restype = C.c_uint64
         L.zc_profile.argtypes = [_vp, C.c_int]
+        L.zc_set_graphs.argtypes = [_vp, C.c_int]
         L.zc_profile_stages.argtypes = [_vp, C.c_uint32, _vp, _vp, _vp, _u32p]
         _lib = L
     return _lib
@@ -176,6 +177,10 @@ class CudaCodec:
 
     def launch_count(self):
         return lib().zc_launch_count(self._ctx)
+
+    def set_graphs(self, on=True):
+        """Capture / replay the device-resident calls as CUDA graphs (keyed by their arguments)."""
+        self._check(lib().zc_set_graphs(self._ctx, 1 if on else 0))
 
     def profile(self, on=True):
         """Per-kernel CUDA-event timing on/off (clears the totals)."""
@@ -269,21 +274,27 @@ class CudaCodec:
         self._check(lib().zc_crc32(self._ctx, _ptr(a), a.size, C.byref(v)))
         return v.value
 
-    # -- device-resident forms (torch CUDA tensors; work queued on `stream`, a raw cudaStream_t handle)
+    # -- device-resident forms (torch CUDA tensors or raw device addresses as ints; work queued on
+    #    `stream`, a raw cudaStream_t handle)
     def compress_device(self, d_in, d_in_offs, d_in_lens, nb, block_log, d_methods, d_lens, d_crcs, d_out,
-                        d_out_offs, d_total, stream=0, level=None):
+                        d_out_offs, d_total, stream=0, level=None, out_cap=None):
         self._check(lib().zc_compress_device(
-            self._ctx, d_in.data_ptr(), d_in_offs.data_ptr(), d_in_lens.data_ptr(), nb, block_log,
-            self.level if level is None else level, d_methods.data_ptr(), d_lens.data_ptr(),
-            d_crcs.data_ptr() if d_crcs is not None else None, d_out.data_ptr(), d_out.numel(),
-            d_out_offs.data_ptr(), d_total.data_ptr(), stream or None))
+            self._ctx, _dp(d_in), _dp(d_in_offs), _dp(d_in_lens), nb, block_log,
+            self.level if level is None else level, _dp(d_methods), _dp(d_lens), _dp(d_crcs), _dp(d_out),
+            out_cap if out_cap is not None else d_out.numel(), _dp(d_out_offs), _dp(d_total), stream or None))
 
     def decompress_device(self, d_comp, d_comp_offs, d_comp_lens, d_methods, d_raw_lens, nb, block_log, d_out,
                           d_out_offs, d_crcs, d_err, stream=0):
         self._check(lib().zc_decompress_device(
-            self._ctx, d_comp.data_ptr(), d_comp_offs.data_ptr(), d_comp_lens.data_ptr(), d_methods.data_ptr(),
-            d_raw_lens.data_ptr(), nb, block_log, d_out.data_ptr(), d_out_offs.data_ptr(),
-            d_crcs.data_ptr() if d_crcs is not None else None, d_err.data_ptr(), stream or None))
+            self._ctx, _dp(d_comp), _dp(d_comp_offs), _dp(d_comp_lens), _dp(d_methods), _dp(d_raw_lens), nb,
+            block_log, _dp(d_out), _dp(d_out_offs), _dp(d_crcs), _dp(d_err), stream or None))
+
+
+def _dp(x):
+    """A device address: an int as given, a tensor's data pointer, None as NULL."""
+    if x is None or isinstance(x, int):
+        return x
+    return x.data_ptr()
 
 
 def crc32_combine(a, b, len_b):
