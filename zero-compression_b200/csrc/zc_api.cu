@@ -127,7 +127,7 @@ struct zc_ctx {
       e_ext, e_sym, e_grp, e_bits, e_lanes, e_freq, e_lanelen, e_sinfo, e_slab;
   // decoder scratch for dec_nb blocks of 2^dec_bl bytes
   uint32_t dec_nb = 0, dec_bl = 0;
-  DevBuf d_lit, d_tok, d_sym, d_grp, d_ext, d_meta;
+  DevBuf d_lit, d_tok, d_sym, d_grp, d_ext, d_meta, d_tks, d_tkm, d_tkd, d_tkl, d_tot;
   // staging for the host-pointer calls
   DevBuf s_in, s_blk, s_out, s_meta;
   HostBuf h_meta;
@@ -220,6 +220,11 @@ int ensure_dec(zc_ctx* c, uint32_t nb, uint32_t block_log) {
   ZC_CUDA(grow(c->d_grp, (size_t)nb * TC));
   ZC_CUDA(grow(c->d_ext, (size_t)nb * EC));
   ZC_CUDA(grow(c->d_meta, (size_t)nb * sizeof(zc::DecMeta)));
+  ZC_CUDA(grow(c->d_tks, (size_t)nb * TC * 4));
+  ZC_CUDA(grow(c->d_tkm, (size_t)nb * TC * 4));
+  ZC_CUDA(grow(c->d_tkd, (size_t)nb * TC * 4));
+  ZC_CUDA(grow(c->d_tkl, (size_t)nb * TC * 4));
+  ZC_CUDA(grow(c->d_tot, (size_t)nb * 8));
   c->dec_nb = nb;
   c->dec_bl = block_log;
   return ZC_OK;
@@ -281,7 +286,9 @@ int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs,
   A.nb = nb; A.B = 1u << block_log; A.out = d_out; A.out_off = d_out_offs; A.err = d_err;
   A.s_lit = c->d_lit.as<uint8_t>(); A.s_tok = c->d_tok.as<uint8_t>(); A.s_sym = c->d_sym.as<uint8_t>();
   A.s_grp = c->d_grp.as<uint8_t>(); A.s_ext = c->d_ext.as<uint8_t>(); A.meta = c->d_meta.as<zc::DecMeta>();
-  zc::launch_decode(A, st, c->stages);
+  A.tk_start = c->d_tks.as<uint32_t>(); A.tk_ms = c->d_tkm.as<uint32_t>(); A.tk_d = c->d_tkd.as<uint32_t>();
+  A.tk_lik = c->d_tkl.as<uint32_t>(); A.tot_op = c->d_tot.as<uint32_t>(); A.tot_li = A.tot_op + nb;
+  zc::launch_decode_fill(A, st, c->stages);
   if (d_crcs && nb) {
     zc::CrcArgs C{};
     C.base = d_out; C.offs = d_out_offs; C.lens = d_raw_lens; C.nb = nb; C.crc = d_crcs; C.err = d_err;
@@ -446,7 +453,7 @@ void zc_close(zc_ctx* c) {
   for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_rank, &c->e_minfo, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
                     &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
                     &c->e_bits, &c->e_lanes, &c->e_freq, &c->e_lanelen, &c->e_sinfo, &c->e_slab, &c->d_lit, &c->d_tok,
-                    &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta})
+                    &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta})
     release(*b);
   if (c->h_meta.p) cudaFreeHost(c->h_meta.p);
   if (c->d_crct) cudaFree(c->d_crct);

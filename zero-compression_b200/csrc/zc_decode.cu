@@ -329,6 +329,10 @@ void launch_decode(const DecArgs& A, cudaStream_t st, Stages& S) {
   S.end(st);
 }
 
+void launch_dec_streams(const DecArgs& A, cudaStream_t st) {
+  if (A.nb) k_dec_streams<<<dim3(A.nb, 5), 64, 0, st>>>(A);
+}
+
 void launch_crc(const CrcArgs& A, cudaStream_t st, Stages& S, const char* name) {
   if (!A.nb) return;
   S.begin(name, st);

@@ -1,0 +1,326 @@
+// zc_decode_fill.cu -- the ZB2 LZ replay in two kernels (src/codec2.h:155-203):
+//
+//   k_dec_tokens  one CTA of 1024 threads per block: every token's literal run and match length (ext
+//                 bytes), offset (offset bits), output start and literal start, from block-wide scans, in
+//                 parallel over the tokens; then one warp resolves the recent-offset symbols (they name
+//                 the offsets of the group before, src/codec2.h:180-192) 32 tokens at a time and checks
+//                 the groups.  Every check of the reference decoder is made here; a failing one records a
+//                 status and the block is not replayed.
+//   k_dec_fill    one warp per block: walks the groups in order and fills each group's output with all
+//                 lanes (a group's matches read only output from before the group, or their own
+//                 literals), the next 32 tokens' table loaded while the current ones are filled.
+// Stored blocks are copied by k_dec_fill.  The rANS streams come from k_dec_streams (zc_decode.cu).
+#include "zc_internal.cuh"
+#include "zc_kernels.h"
+
+namespace zc {
+
+namespace {
+
+__device__ __forceinline__ void flag(uint32_t* err, uint32_t b, uint32_t code) { atomicCAS(err + b, 0u, code); }
+
+// exclusive scan over the CTA (blockDim.x == 1024); returns the prefix, `total` gets the sum.  ws: 32 words
+__device__ __forceinline__ uint32_t cta_scan(uint32_t v, uint32_t* ws, uint32_t& total) {
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  const uint32_t inc = warp_incl_scan(v);
+  if (lane == 31) ws[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const uint32_t x = ws[lane];
+    const uint32_t xi = warp_incl_scan(x);
+    ws[lane] = xi - x;
+    if (lane == 31) ws[32] = xi;
+  }
+  __syncthreads();
+  const uint32_t r = ws[w] + inc - v;
+  total = ws[32];
+  __syncthreads();
+  return r;
+}
+
+constexpr uint32_t kRepMark = 0x80000000u;  // a recent-offset symbol not resolved yet: kRepMark | index
+
+}  // namespace
+
+__global__ void __launch_bounds__(1024) k_dec_tokens(DecArgs A) {
+  const uint32_t b = blockIdx.x, tid = threadIdx.x, lane = tid & 31u;
+  if (A.method[b] != 1 || A.raw_len[b] > A.B || A.err[b]) return;
+  __shared__ uint32_t ws[33];
+  __shared__ uint32_t any_bad;
+  const DecMeta m = A.meta[b];
+  const uint32_t raw = A.raw_len[b], B = A.B;
+  const size_t TC = tok_cap(B), EC = ext_cap(B);
+  const uint8_t* tok = A.s_tok + (size_t)b * TC;
+  const uint8_t* sym = A.s_sym + (size_t)b * TC;
+  const uint8_t* grp = A.s_grp + (size_t)b * TC;
+  const uint8_t* ext = A.s_ext + (size_t)b * EC;
+  const uint8_t* bits = A.comp + A.comp_off[b] + m.bits_off;
+  const uint64_t nbits = 8ull * m.nob;
+  uint32_t* Ts = A.tk_start + (size_t)b * TC;
+  uint32_t* Tm = A.tk_ms + (size_t)b * TC;
+  uint32_t* Td = A.tk_d + (size_t)b * TC;
+  uint32_t* Tl = A.tk_lik + (size_t)b * TC;
+  if (tid == 0) any_bad = 0;
+  __syncthreads();
+  // ---- lengths, offsets and positions, 1024 tokens a tile
+  uint32_t ei = 0, bp = 0, op = 0, li = 0;
+  bool bad = false;
+  for (uint32_t t0 = 0; t0 < m.nt; t0 += 1024) {
+    const uint32_t t = t0 + tid;
+    const bool on = t < m.nt;
+    const uint32_t tv = on ? tok[t] : 0u, sv = on ? sym[t] : 0u;
+    const uint32_t fl = on && (tv >> 4) == 15u, fm = on && (tv & 15u) == 15u;
+    const uint32_t nx = 3u * fl + 2u * fm;
+    const uint32_t nbit = (on && sv <= 19u) ? sv : 0u;
+    if (on && sv > 19u && (sv < kSymRep || sv > kSymRep + 2)) bad = true;
+    uint32_t tsum;
+    const uint32_t pre = cta_scan(nx | nbit << 16, ws, tsum);  // (each part of a tile's sum fits 16 bits)
+    const uint32_t xq = ei + (pre & 0xFFFFu), bq = bp + (pre >> 16);
+    ei += tsum & 0xFFFFu;
+    bp += tsum >> 16;
+    if (on && (uint64_t)xq + nx > m.ne) bad = true;
+    if (on && (uint64_t)bq + nbit > nbits) bad = true;
+    uint32_t L = tv >> 4, M = on ? (tv & 15u) + 4u : 0u;
+    if (!bad && fl) L += (uint32_t)ext[xq] | (uint32_t)ext[xq + 1] << 8 | (uint32_t)ext[xq + 2] << 16;
+    if (!bad && fm) { const uint32_t q = xq + 3u * fl; M += (uint32_t)ext[q] | (uint32_t)ext[q + 1] << 8; }
+    uint32_t D = 0;
+    if (on && !bad) {
+      if (sv >= kSymRep) {
+        D = kRepMark | (sv - kSymRep);
+      } else {
+        uint32_t x = 0;
+        if (nbit) {
+          const uint32_t j0 = bq >> 3, j1 = (bq + nbit - 1) >> 3;
+          uint64_t w = 0;
+          for (uint32_t j = j0; j <= j1; ++j) w |= (uint64_t)bits[j] << (8 * (j - j0));
+          x = (uint32_t)(w >> (bq & 7u)) & ((1u << nbit) - 1u);
+        }
+        D = (1u << sv) + x;
+      }
+    }
+    uint32_t lsum, osum;
+    const uint32_t lpre = cta_scan(L, ws, lsum);
+    const uint32_t opre = cta_scan(L + M, ws, osum);
+    const uint32_t opk = op + opre, lik = li + lpre;
+    if (on && ((uint64_t)lik + L > m.nl || (uint64_t)opk + L + M > raw)) bad = true;
+    if (on) { Ts[t] = opk; Tm[t] = opk + L; Tl[t] = lik; Td[t] = D; }
+    op += osum;
+    li += lsum;
+  }
+  if (bad) any_bad = 1;
+  __syncthreads();
+  // ---- recent offsets and groups, one warp, 32 tokens at a time (as the reference decodes them:
+  //      recent = the last three offsets before the group's first token, src/codec2.h:179, 199)
+  if (tid < 32 && !any_bad) {
+    uint32_t l0 = 1, l1 = 4, l2 = 8, r0 = 1, r1 = 4, r2 = 8, gi = 0, gend = 0;
+    bool wbad = false;
+    for (uint32_t t = 0; t < m.nt && !wbad; t += 32) {
+      const uint32_t c = min(32u, m.nt - t);
+      const bool on = lane < c;
+      const uint32_t gk = gi + lane;
+      const uint32_t gcnt = gk < m.ng ? grp[gk] : 0u;
+      const uint32_t gincl = warp_incl_scan(gcnt);
+      const uint32_t gstart = gend + gincl - gcnt;
+      const bool gin = gk < m.ng && gstart < t + c;
+      bool lbad = gin && gcnt == 0;
+      const uint32_t ngc = __popc(__ballot_sync(kFull, gin));
+      const uint32_t mask = __reduce_or_sync(kFull, gin ? 1u << (gstart - t) : 0u);
+      const uint32_t new_gend = ngc ? __shfl_sync(kFull, gstart + gcnt, ngc - 1) : gend;
+      if (new_gend < t + c || new_gend > m.nt) lbad = true;
+      const unsigned below = mask & (0xFFFFFFFFu >> (31u - lane));
+      const int gsl = below ? 31 - __clz(below) : -1;
+      uint32_t D = on ? Td[t + lane] : 1u;
+      const uint32_t ms = on ? Tm[t + lane] : 0xFFFFFFFFu;
+      bool resolved = !(D & kRepMark);
+      int srcl = (int)lane;
+      if (!resolved) {
+        const uint32_t r = D & 3u;
+        if (gsl < 0) { D = r == 0 ? r0 : r == 1 ? r1 : r2; resolved = true; }
+        else if ((int)r >= gsl) {
+          const uint32_t i = r - (uint32_t)gsl;
+          D = i == 0 ? l0 : i == 1 ? l1 : l2;
+          resolved = true;
+        } else {
+          srcl = gsl - 1 - (int)r;
+        }
+      }
+      for (int it = 0; it < 32 && __any_sync(kFull, !resolved); ++it) {
+        const uint32_t v = __shfl_sync(kFull, D, srcl);
+        const bool rv = __shfl_sync(kFull, resolved, srcl);
+        if (!resolved && rv) { D = v; resolved = true; }
+      }
+      if (on && (!resolved || D == 0 || D > ms)) lbad = true;
+      if (on) Td[t + lane] = D;
+      const int gs_last = __shfl_sync(kFull, gsl, c - 1);
+      if (gs_last >= 0) {
+        uint32_t rec[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const int u = gs_last - 1 - i;
+          const uint32_t v = __shfl_sync(kFull, D, u < 0 ? 0 : u);
+          const int old = -1 - u;
+          rec[i] = u >= 0 ? v : old == 0 ? l0 : old == 1 ? l1 : l2;
+        }
+        r0 = rec[0]; r1 = rec[1]; r2 = rec[2];
+      }
+      for (uint32_t q = c > 3u ? c - 3u : 0u; q < c; ++q) {
+        const uint32_t v = __shfl_sync(kFull, D, q);
+        l2 = l1; l1 = l0; l0 = v;
+      }
+      gi += ngc;
+      gend = new_gend;
+      wbad = __any_sync(kFull, lbad);
+    }
+    if (lane == 0 && (wbad || gend != m.nt || gi != m.ng)) any_bad = 1;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (any_bad || op + (m.nl - li) != raw) flag(A.err, b, E_TOKEN);
+    A.tot_op[b] = op;
+    A.tot_li[b] = li;
+  }
+}
+
+namespace {
+
+// a chunk of at most 32 tokens of one group: output start, match start, offset, literal start;
+// start[c] is the chunk's end
+struct FillTable {
+  uint32_t start[33], ms[32], dist[32], lik[32];
+};
+
+// the byte at output position q of token k: its own literal, or a match byte whose source is output
+// from before the group or the token's own literals; an overlapping match (D < M) repeats the D bytes
+// before it, so match byte i comes from ms - D + (i mod D)
+__device__ __forceinline__ uint32_t fill_byte(const FillTable& T, const uint8_t* o, const uint8_t* lit, uint32_t q,
+                                              uint32_t k) {
+  const uint32_t opk = T.start[k], ms = T.ms[k];
+  if (q < ms) return lit[T.lik[k] + (q - opk)];
+  const uint32_t D = T.dist[k];
+  uint32_t s = q - D;
+  if (s >= ms) s = ms - D + (q - ms) % D;
+  return s >= opk ? lit[T.lik[k] + (s - opk)] : o[s];
+}
+
+// all lanes fill [op, op_end) of c tokens: 4 bytes each per round, aligned words stored as words
+__device__ __forceinline__ void fill_span(const FillTable& T, uint8_t* o, const uint8_t* lit, uint32_t c, uint32_t op,
+                                          uint32_t op_end) {
+  const uintptr_t ob = (uintptr_t)o;
+  const int64_t qa = (int64_t)(((ob + op) & ~(uintptr_t)3) - ob);
+  for (int64_t q0 = qa + 4 * (int64_t)lane_id(); q0 < (int64_t)op_end; q0 += 128) {
+    const uint32_t qs = (uint32_t)(q0 > (int64_t)op ? q0 : (int64_t)op);
+    uint32_t lo = 0, hi = c;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (T.start[mid] <= qs) lo = mid; else hi = mid;
+    }
+    uint32_t k = lo, w = 0;
+    const bool full = q0 >= (int64_t)op && q0 + 4 <= (int64_t)op_end;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t q = q0 + j;
+      if (q < (int64_t)op || q >= (int64_t)op_end) continue;
+      while ((uint32_t)q >= T.start[k + 1]) ++k;
+      const uint32_t v = fill_byte(T, o, lit, (uint32_t)q, k);
+      if (full) w |= v << (8 * j);
+      else o[q] = (uint8_t)v;
+    }
+    if (full) *reinterpret_cast<uint32_t*>(o + q0) = w;
+  }
+}
+
+__device__ inline void copy_bytes(uint8_t* d, const uint8_t* s, uint32_t n) {  // all lanes; no overlap
+  const uint32_t l = lane_id();
+  uint32_t i = 0;
+  if ((((uintptr_t)d ^ (uintptr_t)s) & 15u) == 0) {
+    const uint32_t head = (uint32_t)((16u - ((uintptr_t)d & 15u)) & 15u);
+    if (l < head && l < n) d[l] = s[l];
+    i = head < n ? head : n;
+    for (uint32_t j = i + 16 * l; j + 16 <= n; j += 16 * 32)
+      *reinterpret_cast<uint4*>(d + j) = *reinterpret_cast<const uint4*>(s + j);
+    i += (n - i) & ~15u;
+  }
+  for (uint32_t j = i + l; j < n; j += 32) d[j] = s[j];
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_dec_fill(DecArgs A) {
+  __shared__ FillTable tables[4];
+  const uint32_t b = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (b >= A.nb) return;
+  FillTable& T = tables[threadIdx.x >> 5];
+  const uint32_t lane = lane_id();
+  const uint32_t raw = A.raw_len[b], method = A.method[b], clen = A.comp_len[b], B = A.B;
+  uint8_t* o = A.out + A.out_off[b];
+  const uint8_t* p = A.comp + A.comp_off[b];
+  if (raw > B) { if (lane == 0) flag(A.err, b, E_RAWLEN); return; }
+  if (method == 0) {
+    if (clen != raw) { if (lane == 0) flag(A.err, b, E_STORED); return; }
+    copy_bytes(o, p, raw);
+    return;
+  }
+  if (method != 1) { if (lane == 0) flag(A.err, b, E_METHOD); return; }
+  if (A.err[b]) return;
+  const DecMeta m = A.meta[b];
+  const size_t TC = tok_cap(B);
+  const uint8_t* lit = A.s_lit + (size_t)b * B;
+  const uint8_t* grp = A.s_grp + (size_t)b * TC;
+  const uint32_t* Ts = A.tk_start + (size_t)b * TC;
+  const uint32_t* Tm = A.tk_ms + (size_t)b * TC;
+  const uint32_t* Td = A.tk_d + (size_t)b * TC;
+  const uint32_t* Tl = A.tk_lik + (size_t)b * TC;
+  const uint32_t op_total = A.tot_op[b], li_total = A.tot_li[b];
+  // token windows: lane k holds token w0 + k of the current window, and of the next one (prefetched)
+  uint32_t w0 = 0;
+  auto load = [&](uint32_t base, uint32_t& s, uint32_t& ms, uint32_t& d, uint32_t& l) {
+    const uint32_t t = base + lane;
+    if (t < m.nt) { s = Ts[t]; ms = Tm[t]; d = Td[t]; l = Tl[t]; }
+    else { s = op_total; ms = op_total; d = 1; l = li_total; }
+  };
+  uint32_t cs, cm, cd, cl, ns, nm, nd, nl;
+  load(0, cs, cm, cd, cl);
+  load(32, ns, nm, nd, nl);
+  uint32_t gc = 0;  // the group counts of groups gi0 .. gi0 + 31, lane k holding gi0 + k
+  uint32_t gi0 = 0, t = 0;
+  for (uint32_t g = 0; g < m.ng; ++g) {
+    if ((g & 31u) == 0) { gi0 = g; gc = g + lane < m.ng ? grp[g + lane] : 0u; }
+    const uint32_t gend = t + __shfl_sync(kFull, gc, g - gi0);
+    while (t < gend) {
+      if (t >= w0 + 32) {  // the next window becomes current; prefetch the one after
+        w0 += 32;
+        cs = ns; cm = nm; cd = nd; cl = nl;
+        load(w0 + 32, ns, nm, nd, nl);
+      }
+      const uint32_t k0 = t - w0, k1 = min(gend, w0 + 32) - w0, c = k1 - k0;
+      if (lane >= k0 && lane < k1) {
+        const uint32_t i = lane - k0;
+        T.start[i] = cs; T.ms[i] = cm; T.dist[i] = cd; T.lik[i] = cl;
+      }
+      // the end of the chunk: the next token's start (in this window or the next), or the total
+      const uint32_t e_here = __shfl_sync(kFull, cs, k1 & 31u), e_next = __shfl_sync(kFull, ns, 0);
+      const uint32_t op_end = k1 < 32 ? e_here : e_next;
+      if (lane == 0) T.start[c] = op_end;
+      __syncwarp();
+      fill_span(T, o, lit, c, T.start[0], op_end);
+      __syncwarp();
+      t += c;
+    }
+  }
+  copy_bytes(o + op_total, lit + li_total, m.nl - li_total);
+}
+
+void launch_decode_fill(const DecArgs& A, cudaStream_t st, Stages& S) {
+  if (!A.nb) return;
+  S.begin("k_dec_streams", st);
+  launch_dec_streams(A, st);
+  S.end(st);
+  S.begin("k_dec_tokens", st);
+  k_dec_tokens<<<A.nb, 1024, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_dec_fill", st);
+  k_dec_fill<<<(A.nb + 3) / 4, 128, 0, st>>>(A);
+  S.end(st);
+}
+
+}  // namespace zc

@@ -36,6 +36,10 @@ struct DecArgs {
   // scratch, per block slot b: lit at b*B, tok / sym / grp at b*tok_cap(B), ext at b*ext_cap(B)
   uint8_t *s_lit, *s_tok, *s_sym, *s_grp, *s_ext;
   DecMeta* meta;
+  // the two-kernel replay (launch_decode_fill) only: per token (tok_cap(B) per block) its output start,
+  // match start, offset and literal start; per block the output and literal totals of the tokens
+  uint32_t *tk_start, *tk_ms, *tk_d, *tk_lik;
+  uint32_t *tot_op, *tot_li;
 };
 
 struct CrcArgs {
@@ -49,7 +53,9 @@ struct CrcArgs {
   const CrcTables* tables;
 };
 
-void launch_decode(const DecArgs& A, cudaStream_t st, Stages& S);
+void launch_decode(const DecArgs& A, cudaStream_t st, Stages& S);       // streams + one-kernel replay
+void launch_dec_streams(const DecArgs& A, cudaStream_t st);              // the rANS streams alone
+void launch_decode_fill(const DecArgs& A, cudaStream_t st, Stages& S);  // streams + token scan + fill
 void launch_crc(const CrcArgs& A, cudaStream_t st, Stages& S, const char* name);
 
 // ---- encoder
