@@ -134,6 +134,57 @@ int zc_decompress_noalloc(const uint8_t *d_comp, const uint64_t *d_comp_offs, co
  * and when turned off. */
 int zc_set_graphs(zc_ctx *ctx, int on);
 
+/* ---- serving: a request loop with continuous batching (no reference counterpart; the reference runs
+ * one archive job at a time).  Jobs arrive from any thread; a worker thread admits them in arrival order
+ * while their device memory fits in `budget_bytes` (one arena allocated at open), keeps their bytes and
+ * results on the device, and each tick launches one batch of blocks taken from every admitted job of one
+ * kind, block size and level, so jobs that arrive while others run share the launches.  The batches
+ * have a fixed capacity (padded with empty blocks) and run as CUDA graphs.
+ *
+ * A job:
+ *   ZC_JOB_COMPRESS  in: in_len raw bytes, cut into blocks of 2^block_log, coded at `level`.  Results per
+ *                    block: out_methods, out_lens (payload or raw length), out_crcs, and the ZB2 payloads
+ *                    packed into out (out_cap bytes) at out_offs (stored blocks write nothing).
+ *   ZC_JOB_EXTRACT   in: nb record bodies back to back (comp_lens[b] bytes each, methods[b],
+ *                    raw_lens[b]), as in zc_decompress.  Results: the raw bytes in out, out_crcs.
+ *   ZC_JOB_TEST      as EXTRACT, without returning the bytes: out_crcs, and a damaged status when a block
+ *                    is damaged or its CRC differs from crcs_expected[b] (src/archive.h:747-785).
+ * The caller keeps every buffer of a job alive until zc_serve_wait returns for it. */
+enum { ZC_JOB_COMPRESS = 0, ZC_JOB_EXTRACT = 1, ZC_JOB_TEST = 2 };
+typedef struct {
+  int kind;
+  uint32_t block_log;
+  int level;
+  const uint8_t *in;
+  size_t in_len;
+  uint32_t nb;                     /* EXTRACT / TEST */
+  const uint32_t *comp_lens;       /* EXTRACT / TEST */
+  const uint8_t *methods;          /* EXTRACT / TEST */
+  const uint32_t *raw_lens;        /* EXTRACT / TEST */
+  const uint32_t *crcs_expected;   /* TEST */
+  uint8_t *out;                    /* COMPRESS: payloads; EXTRACT: raw bytes */
+  size_t out_cap;
+  uint8_t *out_methods;            /* COMPRESS */
+  uint32_t *out_lens;              /* COMPRESS */
+  uint64_t *out_offs;              /* COMPRESS */
+  uint32_t *out_crcs;              /* all kinds (may be NULL) */
+} zc_job;
+
+typedef struct zc_server zc_server;
+
+/* Opens a server on `device` with a device arena of budget_bytes for the admitted jobs' data (the
+ * codec's own scratch comes on top).  max_batch_bytes bounds one tick's input (0: the codec's default). */
+int zc_serve_open(zc_server **srv, int device, uint64_t budget_bytes, uint64_t max_batch_bytes);
+/* Waits for every submitted job, then stops the worker and frees the device memory. */
+void zc_serve_close(zc_server *srv);
+/* Queues a job; *id identifies it.  ZC_E_ARG when it could never fit the budget. */
+int zc_serve_submit(zc_server *srv, const zc_job *job, uint64_t *id);
+/* Waits for job `id`; returns its status (ZC_OK, ZC_E_DATA for a damaged block, ...) and, when
+ * latency_s is not NULL, the seconds from its submission to its completion. */
+int zc_serve_wait(zc_server *srv, uint64_t id, double *latency_s);
+/* Counters: jobs done, bytes (raw) processed, ticks, and device bytes in use right now. */
+int zc_serve_stats(zc_server *srv, uint64_t *jobs_done, uint64_t *raw_bytes, uint64_t *ticks, uint64_t *arena_used);
+
 /* CRC-32 of host bytes on the GPU (crc32::of, src/crc32.h:51), and CRC combination on the host
  * (crc32::combine, src/crc32.h:60-66): the CRC of A followed by B. */
 int zc_crc32(zc_ctx *ctx, const uint8_t *data, size_t n, uint32_t *crc);

@@ -1,0 +1,440 @@
+// zc_serve.cu -- the serving loop of include/zero_cuda.h: jobs admitted by free device memory, their
+// blocks batched across jobs tick by tick, each batch one replayed CUDA graph.  Host code only; the work
+// goes through the device entry points (zc_compress_device / zc_decompress_device) of one context.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/zero_cuda.h"
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// first-fit allocation of 256-byte aligned ranges of one device allocation
+struct Arena {
+  uint8_t* base = nullptr;
+  uint64_t size = 0, used = 0;
+  std::map<uint64_t, uint64_t> free_;  // offset -> length
+  static uint64_t round(uint64_t n) { return (n + 255) & ~(uint64_t)255; }
+  bool alloc(uint64_t n, uint64_t& off) {
+    n = round(std::max<uint64_t>(n, 1));
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < n) continue;
+      off = it->first;
+      const uint64_t rest = it->second - n;
+      free_.erase(it);
+      if (rest) free_[off + n] = rest;
+      used += n;
+      return true;
+    }
+    return false;
+  }
+  void release(uint64_t off, uint64_t n) {
+    n = round(std::max<uint64_t>(n, 1));
+    used -= n;
+    auto it = free_.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) { it->second += nx->second; free_.erase(nx); }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) { pv->second += it->second; free_.erase(it); }
+    }
+  }
+};
+
+struct Job {
+  uint64_t id = 0;
+  zc_job j{};
+  double t_submit = 0, t_done = 0;
+  int status = ZC_OK;
+  bool done = false, admitted = false;
+  uint64_t footprint = 0, in_off = 0, out_off = 0;  // arena placement
+  uint32_t nb = 0, next = 0, finished = 0;          // blocks; handed to batches; completed
+  std::vector<uint64_t> bin, bout;                  // per block: input offset, output offset (in the job)
+  std::vector<uint32_t> blen, rlen;                 // per block: input length, raw length
+  uint64_t pay_at = 0;                              // compress: next free byte of the job's payload buffer
+  uint64_t raw_total = 0;
+};
+
+// a batch's class: the kind of kernels, block size and level it shares
+struct Cls {
+  bool compress;
+  uint32_t bl;
+  int level;
+  bool operator==(const Cls& o) const { return compress == o.compress && bl == o.bl && level == o.level; }
+};
+Cls cls_of(const Job* J) {
+  const bool c = J->j.kind == ZC_JOB_COMPRESS;
+  return Cls{c, J->j.block_log, c ? J->j.level : 0};
+}
+
+constexpr uint32_t kCap = 4096;  // blocks per batch at most (padded to a fixed count per block size)
+
+}  // namespace
+
+struct zc_server {
+  int device = 0;
+  zc_ctx* ctx = nullptr;
+  cudaStream_t st = nullptr;
+  Arena arena;
+  uint64_t max_batch = 256ull << 20;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Job*> pending;
+  std::vector<Job*> active;
+  std::map<uint64_t, Job*> jobs;
+  uint64_t next_id = 1;
+  bool stop = false;
+  std::thread worker;
+  uint64_t jobs_done = 0, raw_bytes = 0, ticks = 0;
+  // batch descriptors and results, device and pinned host
+  uint64_t *d_a64 = nullptr, *d_b64 = nullptr, *d_total = nullptr;
+  uint32_t *d_a32 = nullptr, *d_b32 = nullptr, *d_c32 = nullptr, *d_err = nullptr;
+  uint8_t *d_meth = nullptr, *d_stage = nullptr;
+  uint8_t* h = nullptr;  // pinned: descriptors up, results down
+  uint8_t* h_stage = nullptr;
+  int failed = 0;  // a device failure ends the server: every job gets ZC_E_DEVICE
+};
+
+namespace {
+
+uint32_t batch_cap(const zc_server* S, uint32_t bl) {
+  return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(kCap, S->max_batch >> bl));
+}
+
+// places a job in the arena and starts its upload; false when it does not fit now
+bool admit(zc_server* S, Job* J) {
+  uint64_t off;
+  if (!S->arena.alloc(J->footprint, off)) return false;
+  J->in_off = off;
+  J->out_off = off + Arena::round(J->j.in_len + 64);
+  J->admitted = true;
+  if (J->j.in_len) cudaMemcpyAsync(S->arena.base + J->in_off, J->j.in, J->j.in_len, cudaMemcpyHostToDevice, S->st);
+  cudaMemsetAsync(S->arena.base + J->in_off + J->j.in_len, 0, 64, S->st);
+  return true;
+}
+
+void finish(zc_server* S, Job* J, int status) {
+  if (J->done) return;
+  if (status && !J->status) J->status = status;
+  J->done = true;
+  J->t_done = now_s();
+  if (J->admitted) S->arena.release(J->in_off, J->footprint);
+  S->jobs_done += 1;
+  S->raw_bytes += J->raw_total;
+}
+
+// one tick: a batch of blocks of one class, from the admitted jobs in arrival order
+void run_batch(zc_server* S, const Cls& k, std::vector<std::pair<Job*, uint32_t>>& take) {
+  const uint32_t cap = batch_cap(S, k.bl);
+  uint64_t* ha = reinterpret_cast<uint64_t*>(S->h);          // cap: in / comp offsets
+  uint64_t* hb = ha + kCap;                                  // cap: out offsets (decode)
+  uint32_t* h1 = reinterpret_cast<uint32_t*>(hb + kCap);     // cap: lengths (in / comp)
+  uint32_t* h2 = h1 + kCap;                                  // cap: raw lengths (decode)
+  uint8_t* hm = reinterpret_cast<uint8_t*>(h2 + kCap);       // cap: methods
+  // results land after the descriptors
+  uint64_t* r_off = reinterpret_cast<uint64_t*>(hm + kCap);  // cap
+  uint32_t* r_len = reinterpret_cast<uint32_t*>(r_off + kCap);
+  uint32_t* r_crc = r_len + kCap;
+  uint32_t* r_err = r_crc + kCap;
+  uint8_t* r_meth = reinterpret_cast<uint8_t*>(r_err + kCap);
+  uint64_t* r_total = reinterpret_cast<uint64_t*>(r_meth + kCap + 8);
+  const uint32_t n = (uint32_t)take.size();
+  for (uint32_t i = 0; i < cap; ++i) {
+    if (i < n) {
+      Job* J = take[i].first;
+      const uint32_t b = take[i].second;
+      ha[i] = J->in_off + J->bin[b];
+      hb[i] = J->out_off + J->bout[b];
+      h1[i] = J->blen[b];
+      h2[i] = J->rlen[b];
+      hm[i] = k.compress ? 0 : J->j.methods[b];
+    } else {  // padding: an empty block
+      ha[i] = 0; hb[i] = 0; h1[i] = 0; h2[i] = 0; hm[i] = 0;
+    }
+  }
+  cudaStream_t st = S->st;
+  cudaMemcpyAsync(S->d_a64, ha, cap * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(S->d_b64, hb, cap * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(S->d_a32, h1, cap * 4, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(S->d_b32, h2, cap * 4, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(S->d_meth, hm, cap, cudaMemcpyHostToDevice, st);
+  int rc;
+  if (k.compress) {
+    rc = zc_compress_device(S->ctx, S->arena.base, S->d_a64, S->d_a32, cap, k.bl, k.level, S->d_meth, S->d_c32,
+                            S->d_err, S->d_stage, S->max_batch + 64, S->d_b64, S->d_total, st);
+    if (!rc) {
+      cudaMemcpyAsync(r_off, S->d_b64, cap * 8, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(r_len, S->d_c32, cap * 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(r_crc, S->d_err, cap * 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(r_meth, S->d_meth, cap, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(r_total, S->d_total, 8, cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) rc = ZC_E_DEVICE;
+    }
+    if (!rc && *r_total) {
+      cudaMemcpyAsync(S->h_stage, S->d_stage, *r_total, cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) rc = ZC_E_DEVICE;
+    }
+    for (uint32_t i = 0; i < n && !rc; ++i) {
+      Job* J = take[i].first;
+      const uint32_t b = take[i].second;
+      J->j.out_methods[b] = r_meth[i];
+      J->j.out_lens[b] = r_len[i];
+      if (J->j.out_crcs) J->j.out_crcs[b] = r_crc[i];
+      if (r_meth[i]) {
+        if (J->pay_at + r_len[i] > J->j.out_cap) { J->status = ZC_E_ARG; continue; }
+        memcpy(J->j.out + J->pay_at, S->h_stage + r_off[i], r_len[i]);
+        J->j.out_offs[b] = J->pay_at;
+        J->pay_at += r_len[i];
+      } else {
+        J->j.out_offs[b] = 0;
+      }
+    }
+  } else {
+    rc = zc_decompress_device(S->ctx, S->arena.base, S->d_a64, S->d_a32, S->d_meth, S->d_b32, cap, k.bl,
+                              S->arena.base, S->d_b64, S->d_c32, S->d_err, st);
+    if (!rc) {
+      cudaMemcpyAsync(r_crc, S->d_c32, cap * 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(r_err, S->d_err, cap * 4, cudaMemcpyDeviceToHost, st);
+      // the raw bytes of extract jobs, one copy per run of a job's blocks
+      for (uint32_t i = 0; i < n;) {
+        Job* J = take[i].first;
+        uint32_t e = i;
+        while (e < n && take[e].first == J) ++e;
+        if (J->j.kind == ZC_JOB_EXTRACT) {
+          const uint32_t b0 = take[i].second, b1 = take[e - 1].second;
+          const uint64_t o0 = J->bout[b0], o1 = J->bout[b1] + J->rlen[b1];
+          if (o1 > o0) cudaMemcpyAsync(J->j.out + o0, S->arena.base + J->out_off + o0, o1 - o0, cudaMemcpyDeviceToHost, st);
+        }
+        i = e;
+      }
+      if (cudaStreamSynchronize(st) != cudaSuccess) rc = ZC_E_DEVICE;
+    }
+    for (uint32_t i = 0; i < n && !rc; ++i) {
+      Job* J = take[i].first;
+      const uint32_t b = take[i].second;
+      if (J->j.out_crcs) J->j.out_crcs[b] = r_crc[i];
+      if (r_err[i]) J->status = ZC_E_DATA;
+      else if (J->j.kind == ZC_JOB_TEST && J->j.crcs_expected && J->j.crcs_expected[b] != r_crc[i]) J->status = ZC_E_DATA;
+    }
+  }
+  if (rc) S->failed = rc;
+  for (uint32_t i = 0; i < n; ++i) take[i].first->finished += 1;
+}
+
+void worker(zc_server* S) {
+  cudaSetDevice(S->device);
+  std::unique_lock<std::mutex> lk(S->mu);
+  for (;;) {
+    S->cv_work.wait(lk, [&] {
+      if (!S->pending.empty() || S->failed) return true;
+      for (Job* J : S->active) if (J->next < J->nb || J->finished == J->nb) return true;
+      return S->stop && S->active.empty();
+    });
+    if (S->stop && S->pending.empty() && S->active.empty()) return;
+    if (S->failed) {  // the GPU failed: everything left ends with the device error
+      for (Job* J : S->active) finish(S, J, S->failed);
+      for (Job* J : S->pending) finish(S, J, S->failed);
+      S->active.clear();
+      S->pending.clear();
+      S->cv_done.notify_all();
+      if (S->stop) return;
+      S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+      continue;
+    }
+    // admission in arrival order, while the arena has room
+    while (!S->pending.empty() && admit(S, S->pending.front())) {
+      S->active.push_back(S->pending.front());
+      S->pending.pop_front();
+    }
+    // the class of the oldest job with blocks left; then its blocks, and those of later jobs of the class
+    Job* first = nullptr;
+    for (Job* J : S->active) if (J->next < J->nb) { first = J; break; }
+    if (!first) {  // jobs with no blocks at all (empty input) finish at once
+      for (auto it = S->active.begin(); it != S->active.end();) {
+        if ((*it)->finished == (*it)->nb) { finish(S, *it, ZC_OK); it = S->active.erase(it); }
+        else ++it;
+      }
+      S->cv_done.notify_all();
+      continue;
+    }
+    const Cls k = cls_of(first);
+    const uint32_t cap = batch_cap(S, k.bl);
+    std::vector<std::pair<Job*, uint32_t>> take;
+    uint64_t bytes = 0;
+    for (Job* J : S->active) {
+      if (!(cls_of(J) == k)) continue;
+      while (J->next < J->nb && take.size() < cap) {
+        const uint64_t nbytes = (uint64_t)(k.compress ? J->blen[J->next] : J->rlen[J->next]);
+        if (!take.empty() && bytes + nbytes > S->max_batch) break;
+        take.emplace_back(J, J->next++);
+        bytes += nbytes;
+      }
+      if (take.size() >= cap || bytes >= S->max_batch) break;
+    }
+    lk.unlock();
+    run_batch(S, k, take);
+    lk.lock();
+    S->ticks += 1;
+    for (auto it = S->active.begin(); it != S->active.end();) {
+      Job* J = *it;
+      if (J->finished == J->nb) { finish(S, J, ZC_OK); it = S->active.erase(it); }
+      else ++it;
+    }
+    S->cv_done.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int zc_serve_open(zc_server** out, int device, uint64_t budget_bytes, uint64_t max_batch_bytes) {
+  if (!out) return ZC_E_ARG;
+  *out = nullptr;
+  zc_server* S = new zc_server;
+  S->device = device;
+  if (max_batch_bytes) S->max_batch = std::max<uint64_t>(max_batch_bytes, 1u << 20);
+  int rc = zc_open(&S->ctx, device);
+  if (rc) { zc_close(S->ctx); delete S; return rc; }
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&S->arena.base, std::max<uint64_t>(budget_bytes, 1u << 20));
+  if (e == cudaSuccess) {
+    S->arena.size = std::max<uint64_t>(budget_bytes, 1u << 20);
+    S->arena.free_[0] = S->arena.size;
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&S->d_a64, kCap * 8 * 3);
+  if (e == cudaSuccess) { S->d_b64 = S->d_a64 + kCap; S->d_total = S->d_b64 + kCap; }
+  if (e == cudaSuccess) e = cudaMalloc(&S->d_a32, kCap * 4 * 4 + kCap);
+  if (e == cudaSuccess) {
+    S->d_b32 = S->d_a32 + kCap; S->d_c32 = S->d_b32 + kCap; S->d_err = S->d_c32 + kCap;
+    S->d_meth = reinterpret_cast<uint8_t*>(S->d_err + kCap);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&S->d_stage, S->max_batch + 64);
+  if (e == cudaSuccess) e = cudaMallocHost(&S->h, kCap * 64 + 64);
+  if (e == cudaSuccess) e = cudaMallocHost(&S->h_stage, S->max_batch + 64);
+  if (e == cudaSuccess) rc = zc_set_graphs(S->ctx, 1);
+  if (e != cudaSuccess || rc) {
+    zc_serve_close(S);
+    return e == cudaErrorMemoryAllocation ? ZC_E_NOMEM : (rc ? rc : ZC_E_DEVICE);
+  }
+  S->worker = std::thread(worker, S);
+  *out = S;
+  return ZC_OK;
+}
+
+void zc_serve_close(zc_server* S) {
+  if (!S) return;
+  if (S->worker.joinable()) {
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->stop = true;
+    }
+    S->cv_work.notify_all();
+    S->worker.join();
+  }
+  cudaSetDevice(S->device);
+  if (S->st) cudaStreamSynchronize(S->st);
+  for (auto& kv : S->jobs) delete kv.second;
+  if (S->arena.base) cudaFree(S->arena.base);
+  if (S->d_a64) cudaFree(S->d_a64);
+  if (S->d_a32) cudaFree(S->d_a32);
+  if (S->d_stage) cudaFree(S->d_stage);
+  if (S->h) cudaFreeHost(S->h);
+  if (S->h_stage) cudaFreeHost(S->h_stage);
+  if (S->st) cudaStreamDestroy(S->st);
+  zc_close(S->ctx);
+  delete S;
+}
+
+int zc_serve_submit(zc_server* S, const zc_job* job, uint64_t* id) {
+  if (!S || !job || !id) return ZC_E_ARG;
+  const zc_job& j = *job;
+  if (j.block_log < 16 || j.block_log > 20 || (j.in_len && !j.in)) return ZC_E_ARG;
+  Job* J = new Job;
+  J->j = j;
+  const uint64_t B = 1ull << j.block_log;
+  if (j.kind == ZC_JOB_COMPRESS) {
+    if (!j.out_methods || !j.out_lens || !j.out_offs || (j.in_len && (!j.out || j.out_cap < j.in_len))) {
+      delete J;
+      return ZC_E_ARG;
+    }
+    J->nb = (uint32_t)((j.in_len + B - 1) / B);
+    for (uint32_t b = 0; b < J->nb; ++b) {
+      J->bin.push_back((uint64_t)b * B);
+      J->bout.push_back(0);
+      J->blen.push_back((uint32_t)std::min<uint64_t>(B, j.in_len - (uint64_t)b * B));
+      J->rlen.push_back(J->blen.back());
+    }
+    J->raw_total = j.in_len;
+    J->footprint = Arena::round(j.in_len + 64);
+  } else if (j.kind == ZC_JOB_EXTRACT || j.kind == ZC_JOB_TEST) {
+    if (j.nb && (!j.comp_lens || !j.methods || !j.raw_lens)) { delete J; return ZC_E_ARG; }
+    J->nb = j.nb;
+    uint64_t ci = 0, ro = 0;
+    for (uint32_t b = 0; b < j.nb; ++b) {
+      if (j.raw_lens[b] > B) { delete J; return ZC_E_ARG; }
+      J->bin.push_back(ci);
+      J->bout.push_back(ro);
+      J->blen.push_back(j.comp_lens[b]);
+      J->rlen.push_back(j.raw_lens[b]);
+      ci += j.comp_lens[b];
+      ro += j.raw_lens[b];
+    }
+    if (ci > j.in_len || (j.kind == ZC_JOB_EXTRACT && ro && (!j.out || j.out_cap < ro))) { delete J; return ZC_E_ARG; }
+    J->raw_total = ro;
+    J->footprint = Arena::round(j.in_len + 64) + Arena::round(ro + 64);
+  } else {
+    delete J;
+    return ZC_E_ARG;
+  }
+  if (J->footprint > S->arena.size) { delete J; return ZC_E_ARG; }
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    J->id = S->next_id++;
+    J->t_submit = now_s();
+    S->jobs[J->id] = J;
+    S->pending.push_back(J);
+    *id = J->id;
+  }
+  S->cv_work.notify_all();
+  return ZC_OK;
+}
+
+int zc_serve_wait(zc_server* S, uint64_t id, double* latency_s) {
+  if (!S) return ZC_E_ARG;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->jobs.find(id);
+  if (it == S->jobs.end()) return ZC_E_ARG;
+  Job* J = it->second;
+  S->cv_done.wait(lk, [&] { return J->done; });
+  const int st = J->status;
+  if (latency_s) *latency_s = J->t_done - J->t_submit;
+  S->jobs.erase(it);
+  delete J;
+  return st;
+}
+
+int zc_serve_stats(zc_server* S, uint64_t* jobs_done, uint64_t* raw_bytes, uint64_t* ticks, uint64_t* arena_used) {
+  if (!S) return ZC_E_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (jobs_done) *jobs_done = S->jobs_done;
+  if (raw_bytes) *raw_bytes = S->raw_bytes;
+  if (ticks) *ticks = S->ticks;
+  if (arena_used) *arena_used = S->arena.used;
+  return ZC_OK;
+}
+
+}  // extern "C"

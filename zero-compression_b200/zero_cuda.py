@@ -300,3 +300,136 @@ def _dp(x):
 def crc32_combine(a, b, len_b):
     """crc32::combine (src/crc32.h:60-66) on the host."""
     return lib().zc_crc32_combine(a, b, len_b)
+
+
+# ---------------------------------------------------------------- serving (include/zero_cuda.h: zc_serve_*)
+JOB_COMPRESS, JOB_EXTRACT, JOB_TEST = 0, 1, 2
+
+
+class _Job(C.Structure):
+    _fields_ = [("kind", C.c_int), ("block_log", C.c_uint32), ("level", C.c_int), ("in_", C.c_void_p),
+                ("in_len", C.c_size_t), ("nb", C.c_uint32), ("comp_lens", C.c_void_p), ("methods", C.c_void_p),
+                ("raw_lens", C.c_void_p), ("crcs_expected", C.c_void_p), ("out", C.c_void_p),
+                ("out_cap", C.c_size_t), ("out_methods", C.c_void_p), ("out_lens", C.c_void_p),
+                ("out_offs", C.c_void_p), ("out_crcs", C.c_void_p)]
+
+
+class ServeJob:
+    """A submitted job: keeps its buffers alive until waited for; results are filled in place."""
+
+    def __init__(self, kind, arrays):
+        self.kind = kind
+        self.arrays = arrays
+        self.id = None
+        self.status = None
+        self.latency = None
+
+    def __getattr__(self, name):
+        arrays = self.__dict__.get("arrays", {})
+        if name in arrays:
+            return arrays[name]
+        raise AttributeError(name)
+
+
+class Server:
+    """Continuous-batching request loop on one GPU: jobs admitted by free device memory (budget_bytes),
+    their blocks batched with other jobs' blocks tick by tick."""
+
+    def __init__(self, budget_bytes, device=0, max_batch_bytes=0):
+        L = lib()
+        L.zc_serve_open.argtypes = [C.POINTER(_vp), C.c_int, C.c_uint64, C.c_uint64]
+        L.zc_serve_close.argtypes = [_vp]
+        L.zc_serve_submit.argtypes = [_vp, C.POINTER(_Job), C.POINTER(C.c_uint64)]
+        L.zc_serve_wait.argtypes = [_vp, C.c_uint64, C.POINTER(C.c_double)]
+        L.zc_serve_stats.argtypes = [_vp] + [C.POINTER(C.c_uint64)] * 4
+        self._srv = _vp()
+        rc = L.zc_serve_open(C.byref(self._srv), device, budget_bytes, max_batch_bytes)
+        if rc:
+            self._srv = None
+            _raise(None, rc)
+
+    def close(self):
+        if getattr(self, "_srv", None):
+            lib().zc_serve_close(self._srv)
+            self._srv = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _submit(self, job, handle):
+        jid = C.c_uint64()
+        rc = lib().zc_serve_submit(self._srv, C.byref(job), C.byref(jid))
+        if rc:
+            _raise(None, rc)
+        handle.id = jid.value
+        return handle
+
+    def compress(self, data, block_log=18, level=5):
+        a = _as_u8(data)
+        B = 1 << block_log
+        nb = (a.size + B - 1) // B
+        arr = dict(data=a, payloads=np.empty(max(a.size, 1), np.uint8), methods=np.zeros(max(nb, 1), np.uint8),
+                   lens=np.zeros(max(nb, 1), np.uint32), offs=np.zeros(max(nb, 1), np.uint64),
+                   crcs=np.zeros(max(nb, 1), np.uint32))
+        j = _Job(JOB_COMPRESS, block_log, level, _ptr(a), a.size, 0, None, None, None, None, _ptr(arr["payloads"]),
+                 arr["payloads"].size, _ptr(arr["methods"]), _ptr(arr["lens"]), _ptr(arr["offs"]), _ptr(arr["crcs"]))
+        h = ServeJob(JOB_COMPRESS, arr)
+        h.nb = nb
+        return self._submit(j, h)
+
+    def _decode(self, kind, comp, comp_lens, methods, raw_lens, block_log, crcs_expected=None):
+        c = _as_u8(comp)
+        cl = np.ascontiguousarray(comp_lens, np.uint32)
+        me = np.ascontiguousarray(methods, np.uint8)
+        rl = np.ascontiguousarray(raw_lens, np.uint32)
+        nb = rl.size
+        arr = dict(comp=c, comp_lens=cl, methods=me, raw_lens=rl, crcs=np.zeros(max(nb, 1), np.uint32))
+        out = None
+        if kind == JOB_EXTRACT:
+            out = arr["raw"] = np.empty(max(int(rl.sum()), 1), np.uint8)
+        exp = None
+        if crcs_expected is not None:
+            exp = arr["crcs_expected"] = np.ascontiguousarray(crcs_expected, np.uint32)
+        j = _Job(kind, block_log, 0, _ptr(c), c.size, nb, _ptr(cl), _ptr(me), _ptr(rl), _ptr(exp), _ptr(out),
+                 0 if out is None else out.size, None, None, None, _ptr(arr["crcs"]))
+        return self._submit(j, ServeJob(kind, arr))
+
+    def extract(self, comp, comp_lens, methods, raw_lens, block_log=18):
+        """Record bodies back to back -> raw bytes (handle.raw) and CRCs (handle.crcs)."""
+        return self._decode(JOB_EXTRACT, comp, comp_lens, methods, raw_lens, block_log)
+
+    def test(self, comp, comp_lens, methods, raw_lens, crcs_expected, block_log=18):
+        """Decode and check every block's CRC; status DataError on a mismatch."""
+        return self._decode(JOB_TEST, comp, comp_lens, methods, raw_lens, block_log, crcs_expected)
+
+    def wait(self, handle, raise_on_error=True):
+        lat = C.c_double()
+        rc = lib().zc_serve_wait(self._srv, handle.id, C.byref(lat))
+        handle.status, handle.latency = rc, lat.value
+        if rc and raise_on_error:
+            _raise(None, rc)
+        return handle
+
+    def stats(self):
+        v = [C.c_uint64() for _ in range(4)]
+        lib().zc_serve_stats(self._srv, *[C.byref(x) for x in v])
+        return dict(jobs_done=v[0].value, raw_bytes=v[1].value, ticks=v[2].value, arena_used=v[3].value)
+
+
+def record_bodies(data, methods, lens, payloads, offs, block_log):
+    """A compress result as the archive holds it: each block's payload, or its raw bytes when stored;
+    returns (bodies back to back, comp_lens, raw_lens)."""
+    a = _as_u8(data)
+    B = 1 << block_log
+    parts, clens, rlens = [], [], []
+    for b in range(len(methods)):
+        raw = a[b * B:(b + 1) * B]
+        body = payloads[int(offs[b]): int(offs[b]) + int(lens[b])] if methods[b] else raw
+        parts.append(body)
+        clens.append(len(body))
+        rlens.append(raw.size)
+    blob = np.concatenate(parts) if parts else np.zeros(0, np.uint8)
+    return blob, np.array(clens, np.uint32), np.array(rlens, np.uint32)
