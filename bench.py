@@ -635,6 +635,100 @@ def run_decode(args):
     return 0 if ok else 1
 
 
+def run_serve(args):
+    """The serving workload: an open-loop Poisson stream of jobs (60 % compress, 30 % extract, 10 % test),
+    each one file of log-uniform size from the many-file generator mix, block size from {16, 18, 20}, level
+    from {1, 5, 9}, under a device-memory admission budget.  The arrival rate is swept upward until the
+    server saturates; per rate: p50 / p99 latency (submission to completion) and aggregate GB/s."""
+    import threading
+    import queue
+    import numpy as np
+    import zero_cuda as Z
+    import datagen as G
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    rng = np.random.default_rng(4242)
+    pool = []
+    sizes, kinds = G.file_plan(args.pool, 4 << 10, args.max_job_mib << 20, seed=4242)
+    with Z.CudaCodec(level=5, device=local) as codec:
+        for i in range(args.pool):
+            bl = int(rng.choice([16, 18, 20]))
+            lv = int(rng.choice([1, 5, 9]))
+            data = G.by_kind(int(kinds[i]), int(sizes[i]), bl, 8000 + i)
+            meth, lens, crcs, pay, offs = codec.compress_arrays(data, bl, level=lv)
+            blob, clens, rlens = Z.record_bodies(data, meth, lens, pay, offs, bl)
+            pool.append(dict(data=data, bl=bl, lv=lv, blob=blob, clens=clens, meth=meth.copy(), rlens=rlens,
+                             crcs=crcs.copy()))
+    srv = Z.Server(budget_bytes=args.budget_gib << 30, device=local)
+    rates = [float(r) for r in args.rates.split(",")]
+    results = []
+    for rate in rates:
+        done_q = queue.Queue()
+        lat, nbytes, statuses = [], [0], []
+
+        def waiter():
+            while True:
+                h = done_q.get()
+                if h is None:
+                    return
+                srv.wait(h, raise_on_error=False)
+                lat.append(h.latency)
+                statuses.append(h.status)
+                nbytes[0] += h.nbytes
+
+        th = threading.Thread(target=waiter, daemon=True)
+        th.start()
+        t0 = time.perf_counter()
+        t_next = 0.0
+        njobs = 0
+        s0 = srv.stats()
+        while True:
+            t_next += rng.exponential(1.0 / rate)
+            if t_next > args.duration:
+                break
+            delay = t0 + t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            j = pool[int(rng.integers(len(pool)))]
+            u = rng.random()
+            if u < 0.6:
+                h = srv.compress(j["data"], j["bl"], j["lv"])
+                h.nbytes = j["data"].size
+            elif u < 0.9:
+                h = srv.extract(j["blob"], j["clens"], j["meth"], j["rlens"], j["bl"])
+                h.nbytes = int(j["rlens"].sum())
+            else:
+                h = srv.test(j["blob"], j["clens"], j["meth"], j["rlens"], j["crcs"], j["bl"])
+                h.nbytes = int(j["rlens"].sum())
+            done_q.put(h)
+            njobs += 1
+        done_q.put(None)
+        th.join()
+        wall = time.perf_counter() - t0
+        s1 = srv.stats()
+        lat_ms = np.array(lat) * 1e3
+        results.append({"rate_jobs_per_s": rate, "jobs": njobs, "offered_gbs": round(nbytes[0] / args.duration / 1e9, 3),
+                        "achieved_gbs": round(nbytes[0] / wall / 1e9, 3),
+                        "p50_ms": round(float(np.percentile(lat_ms, 50)), 2) if njobs else None,
+                        "p99_ms": round(float(np.percentile(lat_ms, 99)), 2) if njobs else None,
+                        "ticks": s1["ticks"] - s0["ticks"], "errors": int(sum(1 for x in statuses if x)),
+                        "wall_s": round(wall, 2)})
+        print(json.dumps({"serve_rate": results[-1]}), file=sys.stderr, flush=True)
+        if wall > args.duration * 2.0:  # saturated: the backlog took as long again as the arrivals
+            break
+    srv.close()
+    best = max(results, key=lambda r: r["achieved_gbs"])
+    line = {"metric": METRIC, "value": best["achieved_gbs"], "unit": "GB/s", "n_gpus": 1, "higher_is_better": True,
+            "scaling": "weak", "dtype": "u8", "data": "synthetic (seeded per-file generators)",
+            "config": {"workload": f"serving: Poisson jobs 60/30/10 compress/extract/test, sizes log-uniform "
+                                   f"4 KiB-{args.max_job_mib} MiB (pool of {args.pool} files), block 16/18/20, "
+                                   f"level 1/5/9, {args.budget_gib} GiB admission budget, {args.duration} s per rate"},
+            "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "sweep": results}
+    print(json.dumps(line), flush=True)
+    return 0 if all(r["errors"] == 0 for r in results) else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -645,10 +739,15 @@ def main():
     ap.add_argument("--level", type=int, default=5)
     ap.add_argument("--size-mib", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--config", choices=["lz", "batched", "decode"], default="lz",
+    ap.add_argument("--config", choices=["lz", "batched", "decode", "serve"], default="lz",
                     help="lz: the headline round trip; batched: many files, plain vs batched; decode: extract-heavy")
     ap.add_argument("--files", type=int, default=10000)
     ap.add_argument("--max-file-kib", type=int, default=1024)
+    ap.add_argument("--pool", type=int, default=48, help="serve: distinct files the jobs draw from")
+    ap.add_argument("--max-job-mib", type=int, default=256, help="serve: the largest job")
+    ap.add_argument("--budget-gib", type=int, default=112, help="serve: device memory admission budget (GiB)")
+    ap.add_argument("--rates", default="4,8,16,32,64,128", help="serve: arrival rates to sweep (jobs/s)")
+    ap.add_argument("--duration", type=float, default=6.0, help="serve: seconds of arrivals per rate")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -656,6 +755,8 @@ def main():
         return run_batched(args)
     if args.config == "decode":
         return run_decode(args)
+    if args.config == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 
