@@ -134,6 +134,25 @@ int zc_decompress_noalloc(const uint8_t *d_comp, const uint64_t *d_comp_offs, co
  * and when turned off. */
 int zc_set_graphs(zc_ctx *ctx, int on);
 
+/* ---- launch shapes and the autotuner (no reference counterpart: the reference's kernels have fixed
+ * work-group sizes, kernels/zero.cl).  A shape is kept per (block_log, level class: level 1, 2..8, 9)
+ * and never changes a result byte, only speed:
+ *   fill_ring_log   decoder fill: each warp keeps its last 2^fill_ring_log output bytes in shared memory
+ *                   (11..15), so a match nearer than that reads shared instead of global memory
+ *   fill_warps      decoder fill: blocks (warps) per CTA, 1, 2, 4 or 8; fill_warps * (2^fill_ring_log +
+ *                   656) bytes of shared memory per CTA, at most 227 KiB
+ *   match_cap       encoder match pass: bytes compared per candidate before the match is left to the
+ *                   parse to finish, 8..32
+ * The decoder uses the shape of the level last given to zc_prepare (5 by default).  zc_autotune times
+ * the candidates on a host sample (its whole blocks, up to one encoder launch) and keeps the fastest for
+ * (block_log, level); it allocates its own device buffers for the duration of the call. */
+typedef struct zc_shape {
+  uint32_t fill_ring_log, fill_warps, match_cap;
+} zc_shape;
+int zc_get_shape(const zc_ctx *ctx, uint32_t block_log, int level, zc_shape *out);
+int zc_set_shape(zc_ctx *ctx, uint32_t block_log, int level, const zc_shape *shape);
+int zc_autotune(zc_ctx *ctx, const uint8_t *sample, size_t n, uint32_t block_log, int level, zc_shape *chosen);
+
 /* ---- serving: a request loop with continuous batching (no reference counterpart; the reference runs
  * one archive job at a time).  Jobs arrive from any thread; a worker thread admits them in arrival order
  * while their device memory fits in `budget_bytes` (one arena allocated at open), keeps their bytes and

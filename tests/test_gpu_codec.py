@@ -224,3 +224,47 @@ def test_graph_replay_matches_direct(codec):
     codec.set_graphs(False)
     for r in res[1:]:
         assert all(torch.equal(a, b) for a, b in zip(res[0], r))
+
+
+def test_launch_shapes_never_change_bytes(codec):
+    """Every decoder fill shape (ring size, warps per CTA) and encoder match cap gives the
+    same bytes; the autotuner's choice too.  Data with near and far matches, long runs and stored blocks."""
+    import datagen as G
+    default = {bl: codec.get_shape(bl, 5) for bl in (16, 18)}
+    try:
+        for bl in (16, 18):
+            B = 1 << bl
+            data = np.concatenate([G.lz_mix(3 * B + 777, bl, 70 + bl), G.text_mix(B, 71), np.zeros(B // 2, np.uint8),
+                                   G.random_bytes(B // 3, 72), G.lz_mix(B // 2, bl, 73)])
+            ref = cpu_blocks(data.tobytes(), bl, 5)
+            ref_m = [m for m, _ in ref]
+            ref_p = [p for _, p in ref]
+            for cap in (8, 12, 20, 32):
+                codec.set_shape(bl, 5, match_cap=cap)
+                meth, lens, crcs, pay, offs = codec.compress_arrays(data, bl, level=5)
+                assert list(meth) == ref_m, cap
+                for b, p in enumerate(ref_p):
+                    if p is not None:
+                        assert pay[int(offs[b]): int(offs[b]) + int(lens[b])].tobytes() == p, (cap, b)
+            codec.prepare(bl)
+            raw_lens = [min(B, data.size - o) for o in range(0, data.size, B)]
+            comp = [p if p is not None else data[o:o + B].tobytes() for p, o in zip(ref_p, range(0, data.size, B))]
+            coffs = np.cumsum([0] + [len(c) for c in comp[:-1]])
+            for rl in (11, 13, 15):
+                for w in (1, 2, 4, 8):
+                    if w * ((1 << rl) + 656) > 227 * 1024:
+                        continue
+                    codec.set_shape(bl, 5, fill_ring_log=rl, fill_warps=w)
+                    raw, dcrcs, errs = codec.decompress_arrays(b"".join(comp), coffs, [len(c) for c in comp],
+                                                               ref_m, raw_lens)
+                    assert not errs.any() and raw.tobytes() == data.tobytes(), (bl, rl, w)
+            chosen = codec.autotune(data, bl, 5)
+            assert chosen == codec.get_shape(bl, 5)
+            meth, lens, crcs, pay, offs = codec.compress_arrays(data, bl, level=5)
+            assert list(meth) == ref_m
+            raw, _, errs = codec.decompress_arrays(b"".join(comp), coffs, [len(c) for c in comp], ref_m, raw_lens)
+            assert not errs.any() and raw.tobytes() == data.tobytes()
+    finally:
+        for bl, s in default.items():
+            codec.set_shape(bl, 5, **s)
+        codec.prepare(18)

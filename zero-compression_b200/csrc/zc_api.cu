@@ -36,6 +36,7 @@ __global__ void k_plain_blocks(uint64_t n, uint32_t B, uint32_t nb, uint64_t* of
 }
 
 int depth_for_level(int level) { return level <= 1 ? 8 : level >= 9 ? 256 : 32; }
+int level_class(int level) { return level <= 1 ? 0 : level >= 9 ? 2 : 1; }
 
 void build_crc_tables(zc::CrcTables& T) {
   for (uint32_t i = 0; i < 256; ++i) {
@@ -110,8 +111,15 @@ struct GraphEntry {
   uint64_t launches;  // kernels in the graph
 };
 
+// per (block size, level class) launch shapes: the fill's ring and warps per CTA, the match pass's
+// compare cap (none of them changes a result byte)
+struct Shape {
+  uint32_t ring_log = 12, fill_warps = 4, cmp_cap = 32;
+};
+
 struct zc_ctx {
   int device = 0;
+  Shape shape[5][3];
   bool graphs = false;
   std::vector<GraphEntry> graph_cache;
   cudaStream_t stream = nullptr;
@@ -256,7 +264,8 @@ int encode_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_off, const u
   if (int r = ensure_enc(c, nb, block_log)) return r;
   zc::EncArgs A{};
   A.in = d_in; A.in_off = d_off; A.in_len = d_len; A.nb = nb;
-  A.B = 1u << block_log; A.block_log = block_log; A.depth = depth_for_level(level); A.cmp_cap = 32;
+  A.B = 1u << block_log; A.block_log = block_log; A.depth = depth_for_level(level);
+  A.cmp_cap = c->shape[block_log - zc::kMinBlockLog][level_class(level)].cmp_cap;
   A.tmp_pos = c->e_tmp_pos.as<uint32_t>(); A.srt_pos = c->e_srt_pos.as<uint32_t>();
   A.rank = c->e_rank.as<uint32_t>(); A.minfo = c->e_minfo.as<uint32_t>();
   A.tmp_h = c->e_tmp_h.as<uint16_t>(); A.srt_h = c->e_srt_h.as<uint16_t>();
@@ -288,6 +297,8 @@ int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs,
   A.s_grp = c->d_grp.as<uint8_t>(); A.s_ext = c->d_ext.as<uint8_t>(); A.meta = c->d_meta.as<zc::DecMeta>();
   A.tk_start = c->d_tks.as<uint32_t>(); A.tk_ms = c->d_tkm.as<uint32_t>(); A.tk_d = c->d_tkd.as<uint32_t>();
   A.tk_lik = c->d_tkl.as<uint32_t>(); A.tot_op = c->d_tot.as<uint32_t>(); A.tot_li = A.tot_op + nb;
+  const Shape& sh = c->shape[block_log - zc::kMinBlockLog][level_class(c->level)];
+  A.ring_log = sh.ring_log; A.fill_warps = sh.fill_warps;
   zc::launch_decode_fill(A, st, c->stages);
   if (d_crcs && nb) {
     zc::CrcArgs C{};
@@ -569,6 +580,144 @@ int zc_set_graphs(zc_ctx* c, int on) {
   if (!on) drop_graphs(c);
   c->graphs = on != 0;
   return ZC_OK;
+}
+
+int zc_get_shape(const zc_ctx* c, uint32_t block_log, int level, zc_shape* out) {
+  if (!c || !out || bad_block_log(block_log)) return ZC_E_ARG;
+  const Shape& s = c->shape[block_log - zc::kMinBlockLog][level_class(level)];
+  out->fill_ring_log = s.ring_log;
+  out->fill_warps = s.fill_warps;
+  out->match_cap = s.cmp_cap;
+  return ZC_OK;
+}
+
+int zc_set_shape(zc_ctx* c, uint32_t block_log, int level, const zc_shape* in) {
+  if (!c || !in) return ZC_E_ARG;
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  const uint32_t w = in->fill_warps;
+  if (in->fill_ring_log < zc::kMinFillRingLog || in->fill_ring_log > zc::kMaxFillRingLog ||
+      (w != 1 && w != 2 && w != 4 && w != 8) || in->match_cap < 8 ||
+      in->match_cap > 32 || zc::fill_smem_bytes(in->fill_ring_log, w) > zc::kMaxFillSmem)
+    return fail(c, ZC_E_ARG, "launch shape out of range");
+  ZC_CUDA(cudaSetDevice(c->device));
+  Shape& s = c->shape[block_log - zc::kMinBlockLog][level_class(level)];
+  s.ring_log = in->fill_ring_log;
+  s.fill_warps = w;
+  s.cmp_cap = in->match_cap;
+  drop_graphs(c);  // (captured launches carry the old shape)
+  return ZC_OK;
+}
+
+// Times every candidate shape on the sample (whole blocks of it, up to one encoder launch) and keeps
+// the fastest for (block_log, level): the match cap by the encoder's time, the fill's shape by the
+// decoder's.  Each candidate runs once untimed and then `reps` times; its time is the smallest.
+int zc_autotune(zc_ctx* c, const uint8_t* sample, size_t n, uint32_t block_log, int level, zc_shape* chosen) {
+  if (!c || (!sample && n)) return ZC_E_ARG;
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  if (!n) return fail(c, ZC_E_ARG, "autotuning needs a sample");
+  ZC_CUDA(cudaSetDevice(c->device));
+  const uint64_t B = 1ull << block_log;
+  uint32_t nb = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(n / B, 1), enc_blocks_per_launch(block_log));
+  const uint64_t used = std::min<uint64_t>(n, (uint64_t)nb * B);
+  nb = (uint32_t)((used + B - 1) / B);
+  cudaStream_t st = c->stream;
+  const size_t per_blk = 8 + 4 + 1 + 4 + 4 + 8 + 4 + 8;
+  const size_t need = used + 64 + 2 * ((size_t)nb * B + 64) + (size_t)nb * per_blk + 16 * 256;  // (+ rounding)
+  DevBuf tb;
+  ZC_CUDA(grow(tb, need));
+  uint8_t* p = tb.as<uint8_t>();
+  auto take = [&](size_t bytes) { uint8_t* q = p; p += (bytes + 255) & ~(size_t)255; return q; };
+  uint8_t* d_in = take(used + 64);
+  uint8_t* d_comp = take((size_t)nb * B + 64);
+  uint8_t* d_raw = take((size_t)nb * B + 64);
+  uint64_t* d_ioff = reinterpret_cast<uint64_t*>(take((size_t)nb * 8));
+  uint32_t* d_ilen = reinterpret_cast<uint32_t*>(take((size_t)nb * 4));
+  uint8_t* d_meth = take(nb);
+  uint32_t* d_clen = reinterpret_cast<uint32_t*>(take((size_t)nb * 4));
+  uint32_t* d_crc = reinterpret_cast<uint32_t*>(take((size_t)nb * 4));
+  uint64_t* d_coff = reinterpret_cast<uint64_t*>(take((size_t)nb * 8));
+  uint32_t* d_err = reinterpret_cast<uint32_t*>(take((size_t)nb * 4));
+  uint64_t* d_tot = reinterpret_cast<uint64_t*>(take(8));
+  std::vector<uint64_t> ioff(nb);
+  std::vector<uint32_t> ilen(nb);
+  for (uint32_t b = 0; b < nb; ++b) {
+    ioff[b] = (uint64_t)b * B;
+    ilen[b] = (uint32_t)std::min<uint64_t>(B, used - ioff[b]);
+  }
+  int r = ZC_OK;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  const bool timing = c->stages.timing;
+  c->stages.timing = false;
+  Shape& cur = c->shape[block_log - zc::kMinBlockLog][level_class(level)];
+  const Shape saved = cur;
+  const int saved_level = c->level;
+  c->level = level;
+  const int reps = 3;
+  auto timed = [&](auto&& run, float& best_ms) -> int {
+    best_ms = 1e30f;
+    if (int q = run()) return q;
+    for (int i = 0; i < reps; ++i) {
+      cudaEventRecord(e0, st);
+      if (int q = run()) return q;
+      cudaEventRecord(e1, st);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) return cuda_fail(c, e, "autotune timing");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      best_ms = std::min(best_ms, ms);
+    }
+    return ZC_OK;
+  };
+  auto encode = [&]() {
+    return encode_device(c, d_in, d_ioff, d_ilen, nb, block_log, level, d_meth, d_clen, d_crc, d_comp, (size_t)nb * B,
+                         d_coff, d_tot, 1, st);
+  };
+  auto decode = [&]() {
+    return decode_device(c, d_comp, d_coff, d_clen, d_meth, d_ilen, nb, block_log, d_raw, d_ioff, nullptr, d_err, st);
+  };
+  do {
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_in, sample, used, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ioff, ioff.data(), (size_t)nb * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ilen, ilen.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { r = cuda_fail(c, e, "autotune set-up"); break; }
+    Shape best = saved;
+    float best_ms = 1e30f;
+    for (uint32_t cap : {12u, 16u, 20u, 24u, 28u, 32u}) {
+      cur = best;
+      cur.cmp_cap = cap;
+      float ms;
+      if ((r = timed(encode, ms))) break;
+      if (ms < best_ms) { best_ms = ms; best.cmp_cap = cap; }
+    }
+    if (r) break;
+    cur = best;
+    if ((r = encode())) break;  // (every cap writes the same payloads)
+    best_ms = 1e30f;
+    for (uint32_t rl = 11; rl <= 14 && !r; ++rl)
+      for (uint32_t w : {1u, 2u, 4u, 8u}) {
+        if (zc::fill_smem_bytes(rl, w) > zc::kMaxFillSmem) continue;
+        Shape s = best;
+        s.ring_log = rl; s.fill_warps = w;
+        cur = s;
+        float ms;
+        if ((r = timed(decode, ms))) break;
+        if (ms < best_ms) { best_ms = ms; best.ring_log = rl; best.fill_warps = w; }
+      }
+    if (r) break;
+    cur = best;
+  } while (false);
+  if (r) cur = saved;
+  c->level = saved_level;
+  c->stages.timing = timing;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaStreamSynchronize(st);
+  release(tb);
+  drop_graphs(c);
+  if (!r && chosen) r = zc_get_shape(c, block_log, level, chosen);
+  return r;
 }
 
 int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, const uint32_t* comp_lens,

@@ -183,49 +183,85 @@ __global__ void __launch_bounds__(1024) k_dec_tokens(DecArgs A) {
 
 namespace {
 
-// a chunk of at most 32 tokens of one group: output start, match start, offset, literal start;
-// start[c] is the chunk's end
+// a chunk of at most 32 tokens of one group: start[i] the output start of token i (start[c] the chunk's
+// end); tk[i] = {match start, literal start - output start (mod 2^32), offset D, the reciprocal
+// ceil(2^32 / D) when the match overlaps itself (D < M, D >= 2), else 0}
 struct FillTable {
-  uint32_t start[33], ms[32], dist[32], lik[32];
+  uint32_t start[33];
+  uint32_t pad_[3];
+  uint4 tk[32];
 };
+constexpr uint32_t kTableBytes = (sizeof(FillTable) + 15u) & ~15u;
 
-// the byte at output position q of token k: its own literal, or a match byte whose source is output
-// from before the group or the token's own literals; an overlapping match (D < M) repeats the D bytes
-// before it, so match byte i comes from ms - D + (i mod D)
-__device__ __forceinline__ uint32_t fill_byte(const FillTable& T, const uint8_t* o, const uint8_t* lit, uint32_t q,
-                                              uint32_t k) {
-  const uint32_t opk = T.start[k], ms = T.ms[k];
-  if (q < ms) return lit[T.lik[k] + (q - opk)];
-  const uint32_t D = T.dist[k];
-  uint32_t s = q - D;
-  if (s >= ms) s = ms - D + (q - ms) % D;
-  return s >= opk ? lit[T.lik[k] + (s - opk)] : o[s];
-}
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
-// all lanes fill [op, op_end) of c tokens: 4 bytes each per round, aligned words stored as words
-__device__ __forceinline__ void fill_span(const FillTable& T, uint8_t* o, const uint8_t* lit, uint32_t c, uint32_t op,
-                                          uint32_t op_end) {
-  const uintptr_t ob = (uintptr_t)o;
-  const int64_t qa = (int64_t)(((ob + op) & ~(uintptr_t)3) - ob);
-  for (int64_t q0 = qa + 4 * (int64_t)lane_id(); q0 < (int64_t)op_end; q0 += 128) {
-    const uint32_t qs = (uint32_t)(q0 > (int64_t)op ? q0 : (int64_t)op);
-    uint32_t lo = 0, hi = c;
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (T.start[mid] <= qs) lo = mid; else hi = mid;
-    }
-    uint32_t k = lo, w = 0;
-    const bool full = q0 >= (int64_t)op && q0 + 4 <= (int64_t)op_end;
+// Fills [op, op_end) of the chunk's tokens, 4 bytes a lane per round of 128 bytes, each lane's word
+// aligned in memory.  A token is at least 4 bytes long, so an aligned word holds at most one token
+// start: a round's starts form a 32-bit word mask (one OR-reduction over the window lanes `cs` of
+// chunk tokens k0 .. k1-1), and a lane's bytes belong to the last token starting at or before its word,
+// or the one before that.  A byte is its token's literal, or a match byte whose source is output from
+// before the group or the token's own literals (an overlapping match, D < M, repeats the D bytes before
+// it: match byte i comes from ms - D + (i mod D), the quotient from a multiply-high by the reciprocal,
+// exact to one step, which a compare corrects).  Output from before the group is read from the warp's
+// ring of the last R output bytes (shared memory, indexed by address mod R) when the round's own stores
+// cannot have replaced it, else from global memory.  A round's loads are all issued before its stores.
+__device__ __forceinline__ void fill_span(const FillTable& T, uint8_t* o, uint8_t* ring, uint32_t rmask,
+                                          const uint8_t* lit, uint32_t op, uint32_t op_end, uint32_t cs, uint32_t k0,
+                                          uint32_t k1) {
+  const uint32_t lane = lane_id();
+  const uint32_t ob = (uint32_t)(uintptr_t)o;
+  const bool mine = lane >= k0 && lane < k1;
+  uint32_t kb = 0;  // chunk tokens starting before the round
+  for (int32_t base = (int32_t)op - (int32_t)((ob + op) & 3u); base < (int32_t)op_end; base += 128) {
+    const int32_t rel = (int32_t)cs - base;
+    const uint32_t mask = __reduce_or_sync(kFull, mine && rel >= 0 && rel < 128 ? 1u << (rel >> 2) : 0u);
+    const uint32_t cnt = kb + __popc(mask & (0xFFFFFFFFu >> (31u - lane)));
+    kb += __popc(mask);
+    const int32_t q0 = base + 4 * (int32_t)lane;
+    if (q0 >= (int32_t)op_end || q0 + 4 <= (int32_t)op) continue;
+    const int32_t b1 = base + 128 < (int32_t)op_end ? base + 128 : (int32_t)op_end;
+    const int32_t rlo = b1 - (int32_t)(rmask + 1);  // ring bytes at or after rlo survive this round's stores
+    const uint32_t i1 = cnt - 1, i0 = cnt >= 2 ? cnt - 2 : 0;
+    const uint32_t st1 = T.start[i1], st0 = T.start[i0];
+    const uint4 t1 = T.tk[i1], t0 = T.tk[i0];
+    const uint8_t* src[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int64_t q = q0 + j;
-      if (q < (int64_t)op || q >= (int64_t)op_end) continue;
-      while ((uint32_t)q >= T.start[k + 1]) ++k;
-      const uint32_t v = fill_byte(T, o, lit, (uint32_t)q, k);
-      if (full) w |= v << (8 * j);
-      else o[q] = (uint8_t)v;
+      const uint32_t q = (uint32_t)(q0 + j);
+      const bool h = q >= st1;
+      const uint32_t opk = h ? st1 : st0, ms = h ? t1.x : t0.x, ld = h ? t1.y : t0.y, D = h ? t1.z : t0.z,
+                     mg = h ? t1.w : t0.w;
+      const uint8_t* p;
+      if (q < ms) {
+        p = lit + (q + ld);
+      } else {
+        uint32_t s = q - D;
+        if (s >= ms) {
+          const uint32_t x = q - ms;
+          uint32_t r = mg ? x - __umulhi(x, mg) * D : 0u;
+          if ((int32_t)r < 0) r += D;
+          s = ms - D + r;
+        }
+        p = s >= opk ? lit + (s + ld) : (int32_t)s >= rlo ? ring + ((ob + s) & rmask) : o + s;
+      }
+      src[j] = (int32_t)q >= (int32_t)op && q < op_end ? p : ring;
     }
-    if (full) *reinterpret_cast<uint32_t*>(o + q0) = w;
+    uint32_t w = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) w |= (uint32_t)*src[j] << (8 * j);
+    uint8_t* rq = ring + ((ob + (uint32_t)q0) & rmask);
+    if (q0 >= (int32_t)op && q0 + 4 <= (int32_t)op_end) {
+      *reinterpret_cast<uint32_t*>(o + q0) = w;
+      *reinterpret_cast<uint32_t*>(rq) = w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int32_t q = q0 + j;
+        if (q < (int32_t)op || q >= (int32_t)op_end) continue;
+        o[q] = (uint8_t)(w >> (8 * j));
+        rq[j] = (uint8_t)(w >> (8 * j));
+      }
+    }
   }
 }
 
@@ -245,11 +281,16 @@ __device__ inline void copy_bytes(uint8_t* d, const uint8_t* s, uint32_t n) {  /
 
 }  // namespace
 
-__global__ void __launch_bounds__(128) k_dec_fill(DecArgs A) {
-  __shared__ FillTable tables[4];
-  const uint32_t b = blockIdx.x * 4 + (threadIdx.x >> 5);
+// One warp per block; a CTA holds blockDim.x / 32 warps, each with its table and a ring of 2^ring_log
+// bytes in dynamic shared memory (16-byte aligned, the ring after the table).
+__global__ void __launch_bounds__(256) k_dec_fill(DecArgs A) {
+  extern __shared__ __align__(16) uint8_t fsm[];
+  const uint32_t R = 1u << A.ring_log;
+  const uint32_t wid = threadIdx.x >> 5;
+  const uint32_t b = blockIdx.x * (blockDim.x >> 5) + wid;
   if (b >= A.nb) return;
-  FillTable& T = tables[threadIdx.x >> 5];
+  FillTable& T = *reinterpret_cast<FillTable*>(fsm + (size_t)wid * (kTableBytes + R));
+  uint8_t* ring = fsm + (size_t)wid * (kTableBytes + R) + kTableBytes;
   const uint32_t lane = lane_id();
   const uint32_t raw = A.raw_len[b], method = A.method[b], clen = A.comp_len[b], B = A.B;
   uint8_t* o = A.out + A.out_off[b];
@@ -271,16 +312,22 @@ __global__ void __launch_bounds__(128) k_dec_fill(DecArgs A) {
   const uint32_t* Td = A.tk_d + (size_t)b * TC;
   const uint32_t* Tl = A.tk_lik + (size_t)b * TC;
   const uint32_t op_total = A.tot_op[b], li_total = A.tot_li[b];
-  // token windows: lane k holds token w0 + k of the current window, and of the next one (prefetched)
+  // token windows: lane k holds token w0 + k of the current window, and of the next one (prefetched;
+  // a match whose source lies beyond the ring has its first source line brought into L2 then)
   uint32_t w0 = 0;
   auto load = [&](uint32_t base, uint32_t& s, uint32_t& ms, uint32_t& d, uint32_t& l) {
     const uint32_t t = base + lane;
-    if (t < m.nt) { s = Ts[t]; ms = Tm[t]; d = Td[t]; l = Tl[t]; }
-    else { s = op_total; ms = op_total; d = 1; l = li_total; }
+    if (t < m.nt) {
+      s = Ts[t]; ms = Tm[t]; d = Td[t]; l = Tl[t];
+      if (d >= R) prefetch_l2(o + (ms - d));
+    } else {
+      s = op_total; ms = op_total; d = 1; l = li_total;
+    }
   };
   uint32_t cs, cm, cd, cl, ns, nm, nd, nl;
   load(0, cs, cm, cd, cl);
   load(32, ns, nm, nd, nl);
+  const uint32_t rmask = R - 1;
   uint32_t gc = 0;  // the group counts of groups gi0 .. gi0 + 31, lane k holding gi0 + k
   uint32_t gi0 = 0, t = 0;
   for (uint32_t g = 0; g < m.ng; ++g) {
@@ -293,21 +340,33 @@ __global__ void __launch_bounds__(128) k_dec_fill(DecArgs A) {
         load(w0 + 32, ns, nm, nd, nl);
       }
       const uint32_t k0 = t - w0, k1 = min(gend, w0 + 32) - w0, c = k1 - k0;
+      // each token's end: the next token's start (in this window or the next), or the total
+      const uint32_t e_next = __shfl_sync(kFull, ns, 0);
+      const uint32_t e_dn = __shfl_down_sync(kFull, cs, 1);
+      const uint32_t tend = lane < 31 ? e_dn : e_next;
       if (lane >= k0 && lane < k1) {
         const uint32_t i = lane - k0;
-        T.start[i] = cs; T.ms[i] = cm; T.dist[i] = cd; T.lik[i] = cl;
+        const uint32_t mg = cd >= 2 && cd < tend - cm ? 0xFFFFFFFFu / cd + 1u : 0u;
+        T.start[i] = cs;
+        T.tk[i] = make_uint4(cm, cl - cs, cd, mg);
       }
-      // the end of the chunk: the next token's start (in this window or the next), or the total
-      const uint32_t e_here = __shfl_sync(kFull, cs, k1 & 31u), e_next = __shfl_sync(kFull, ns, 0);
-      const uint32_t op_end = k1 < 32 ? e_here : e_next;
+      const uint32_t op_end = __shfl_sync(kFull, tend, k1 - 1);
+      const uint32_t op = __shfl_sync(kFull, cs, k0);
       if (lane == 0) T.start[c] = op_end;
       __syncwarp();
-      fill_span(T, o, lit, c, T.start[0], op_end);
+      fill_span(T, o, ring, rmask, lit, op, op_end, cs, k0, k1);
       __syncwarp();
       t += c;
     }
   }
   copy_bytes(o + op_total, lit + li_total, m.nl - li_total);
+}
+
+size_t fill_smem_bytes(uint32_t ring_log, uint32_t warps) { return (size_t)warps * (kTableBytes + (1u << ring_log)); }
+
+cudaError_t prepare_fill() {
+  const int cap = (int)kMaxFillSmem;
+  return cudaFuncSetAttribute(k_dec_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
 }
 
 void launch_decode_fill(const DecArgs& A, cudaStream_t st, Stages& S) {
@@ -318,8 +377,10 @@ void launch_decode_fill(const DecArgs& A, cudaStream_t st, Stages& S) {
   S.begin("k_dec_tokens", st);
   k_dec_tokens<<<A.nb, 1024, 0, st>>>(A);
   S.end(st);
+  const uint32_t W = A.fill_warps;
+  const size_t sm = fill_smem_bytes(A.ring_log, W);
   S.begin("k_dec_fill", st);
-  k_dec_fill<<<(A.nb + 3) / 4, 128, 0, st>>>(A);
+  k_dec_fill<<<(A.nb + W - 1) / W, 32 * W, sm, st>>>(A);
   S.end(st);
 }
 

@@ -733,7 +733,8 @@ __global__ void __launch_bounds__(256) k_enc_emit(EncArgs A) {
 }
 
 cudaError_t prepare_kernels() {  // with the device current, once per context
-  return cudaFuncSetAttribute(k_enc_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmem);
+  cudaError_t e = cudaFuncSetAttribute(k_enc_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmem);
+  return e == cudaSuccess ? prepare_fill() : e;
 }
 
 void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Stages& S) {

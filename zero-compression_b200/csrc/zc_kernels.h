@@ -40,7 +40,13 @@ struct DecArgs {
   // match start, offset and literal start; per block the output and literal totals of the tokens
   uint32_t *tk_start, *tk_ms, *tk_d, *tk_lik;
   uint32_t *tot_op, *tot_li;
+  // the fill's shape: a ring of 2^ring_log recent output bytes per warp, fill_warps warps (blocks) per CTA
+  uint32_t ring_log, fill_warps;
 };
+
+constexpr uint32_t kMinFillRingLog = 11, kMaxFillRingLog = 15, kMaxFillWarps = 8;
+constexpr size_t kMaxFillSmem = 227 * 1024;
+size_t fill_smem_bytes(uint32_t ring_log, uint32_t warps);
 
 struct CrcArgs {
   const uint8_t* base;
@@ -104,6 +110,7 @@ __host__ __device__ inline uint64_t lanes_per_block(uint32_t B) { return lane_ba
 __host__ __device__ inline uint32_t bits_cap(uint32_t B) { return 5 * B / 8 + 64; }
 
 void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Stages& S);
-cudaError_t prepare_kernels();  // per-kernel attributes (the sort's shared memory), the device current
+cudaError_t prepare_kernels();
+cudaError_t prepare_fill();  // per-kernel attributes (the sort's shared memory), the device current
 
 }  // namespace zc

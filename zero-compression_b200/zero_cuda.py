@@ -87,9 +87,20 @@ def lib():
         L.zc_launch_count.restype = C.c_uint64
         L.zc_profile.argtypes = [_vp, C.c_int]
         L.zc_set_graphs.argtypes = [_vp, C.c_int]
+        L.zc_get_shape.argtypes = [_vp, C.c_uint32, C.c_int, C.POINTER(Shape)]
+        L.zc_set_shape.argtypes = [_vp, C.c_uint32, C.c_int, C.POINTER(Shape)]
+        L.zc_autotune.argtypes = [_vp, _vp, C.c_size_t, C.c_uint32, C.c_int, C.POINTER(Shape)]
         L.zc_profile_stages.argtypes = [_vp, C.c_uint32, _vp, _vp, _vp, _u32p]
         _lib = L
     return _lib
+
+
+class Shape(C.Structure):
+    """zc_shape: launch shapes kept per (block_log, level class); none of them changes a result byte."""
+    _fields_ = [("fill_ring_log", C.c_uint32), ("fill_warps", C.c_uint32), ("match_cap", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
 def _ptr(a):
@@ -181,6 +192,26 @@ class CudaCodec:
     def set_graphs(self, on=True):
         """Capture / replay the device-resident calls as CUDA graphs (keyed by their arguments)."""
         self._check(lib().zc_set_graphs(self._ctx, 1 if on else 0))
+
+    def get_shape(self, block_log, level):
+        s = Shape()
+        self._check(lib().zc_get_shape(self._ctx, block_log, level, C.byref(s)))
+        return s.as_dict()
+
+    def set_shape(self, block_log, level, **kw):
+        """Sets some fields of the (block_log, level) shape; returns the new shape."""
+        s = Shape(**self.get_shape(block_log, level))
+        for k, v in kw.items():
+            setattr(s, k, int(v))
+        self._check(lib().zc_set_shape(self._ctx, block_log, level, C.byref(s)))
+        return s.as_dict()
+
+    def autotune(self, sample, block_log, level):
+        """Times the candidate shapes on `sample` (numpy u8) and keeps the fastest; returns it."""
+        a = np.ascontiguousarray(sample, dtype=np.uint8)
+        s = Shape()
+        self._check(lib().zc_autotune(self._ctx, a.ctypes.data, a.size, block_log, level, C.byref(s)))
+        return s.as_dict()
 
     def profile(self, on=True):
         """Per-kernel CUDA-event timing on/off (clears the totals)."""
