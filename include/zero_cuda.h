@@ -143,11 +143,12 @@ int zc_set_graphs(zc_ctx *ctx, int on);
  *                   656) bytes of shared memory per CTA, at most 227 KiB
  *   match_cap       encoder match pass: bytes compared per candidate before the match is left to the
  *                   parse to finish, 8..32
+ *   match_tile      encoder match pass: sorted positions per CTA of 256 threads (256, 512 or 1024)
  * The decoder uses the shape of the level last given to zc_prepare (5 by default).  zc_autotune times
  * the candidates on a host sample (its whole blocks, up to one encoder launch) and keeps the fastest for
  * (block_log, level); it allocates its own device buffers for the duration of the call. */
 typedef struct zc_shape {
-  uint32_t fill_ring_log, fill_warps, match_cap;
+  uint32_t fill_ring_log, fill_warps, match_cap, match_tile;
 } zc_shape;
 int zc_get_shape(const zc_ctx *ctx, uint32_t block_log, int level, zc_shape *out);
 int zc_set_shape(zc_ctx *ctx, uint32_t block_log, int level, const zc_shape *shape);

@@ -239,13 +239,13 @@ def test_launch_shapes_never_change_bytes(codec):
             ref = cpu_blocks(data.tobytes(), bl, 5)
             ref_m = [m for m, _ in ref]
             ref_p = [p for _, p in ref]
-            for cap in (8, 12, 20, 32):
-                codec.set_shape(bl, 5, match_cap=cap)
+            for cap, tile in ((8, 256), (12, 1024), (20, 512), (32, 256), (32, 1024)):
+                codec.set_shape(bl, 5, match_cap=cap, match_tile=tile)
                 meth, lens, crcs, pay, offs = codec.compress_arrays(data, bl, level=5)
-                assert list(meth) == ref_m, cap
+                assert list(meth) == ref_m, (cap, tile)
                 for b, p in enumerate(ref_p):
                     if p is not None:
-                        assert pay[int(offs[b]): int(offs[b]) + int(lens[b])].tobytes() == p, (cap, b)
+                        assert pay[int(offs[b]): int(offs[b]) + int(lens[b])].tobytes() == p, (cap, tile, b)
             codec.prepare(bl)
             raw_lens = [min(B, data.size - o) for o in range(0, data.size, B)]
             comp = [p if p is not None else data[o:o + B].tobytes() for p, o in zip(ref_p, range(0, data.size, B))]

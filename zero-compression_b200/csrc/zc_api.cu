@@ -114,7 +114,7 @@ struct GraphEntry {
 // per (block size, level class) launch shapes: the fill's ring and warps per CTA, the match pass's
 // compare cap (none of them changes a result byte)
 struct Shape {
-  uint32_t ring_log = 12, fill_warps = 4, cmp_cap = 32;
+  uint32_t ring_log = 12, fill_warps = 4, cmp_cap = 16, match_tile = 1024;
 };
 
 struct zc_ctx {
@@ -131,7 +131,7 @@ struct zc_ctx {
   zc::CrcTables* d_crct = nullptr;
   // encoder scratch for enc_nb blocks of 2^enc_bl bytes
   uint32_t enc_nb = 0, enc_bl = 0;
-  DevBuf e_tmp_pos, e_srt_pos, e_rank, e_minfo, e_tmp_h, e_srt_h, e_tk_i, e_tk_m, e_tk_d, e_bcnt, e_lit, e_tok,
+  DevBuf e_tmp_pos, e_srt_pos, e_minfo, e_tmp_h, e_srt_h, e_tk_i, e_tk_m, e_tk_d, e_bcnt, e_lit, e_tok,
       e_ext, e_sym, e_grp, e_bits, e_lanes, e_freq, e_lanelen, e_sinfo, e_slab;
   // decoder scratch for dec_nb blocks of 2^dec_bl bytes
   uint32_t dec_nb = 0, dec_bl = 0;
@@ -194,7 +194,6 @@ int ensure_enc(zc_ctx* c, uint32_t nb, uint32_t block_log) {
   const size_t N = (size_t)nb * B;
   ZC_CUDA(grow(c->e_tmp_pos, N * 4));
   ZC_CUDA(grow(c->e_srt_pos, N * 4));
-  ZC_CUDA(grow(c->e_rank, N * 4));
   ZC_CUDA(grow(c->e_minfo, N * 4));
   ZC_CUDA(grow(c->e_tmp_h, N * 2));
   ZC_CUDA(grow(c->e_srt_h, N * 2));
@@ -265,9 +264,11 @@ int encode_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_off, const u
   zc::EncArgs A{};
   A.in = d_in; A.in_off = d_off; A.in_len = d_len; A.nb = nb;
   A.B = 1u << block_log; A.block_log = block_log; A.depth = depth_for_level(level);
-  A.cmp_cap = c->shape[block_log - zc::kMinBlockLog][level_class(level)].cmp_cap;
+  const Shape& sh = c->shape[block_log - zc::kMinBlockLog][level_class(level)];
+  A.cmp_cap = sh.cmp_cap;
+  A.match_tile = sh.match_tile;
   A.tmp_pos = c->e_tmp_pos.as<uint32_t>(); A.srt_pos = c->e_srt_pos.as<uint32_t>();
-  A.rank = c->e_rank.as<uint32_t>(); A.minfo = c->e_minfo.as<uint32_t>();
+  A.minfo = c->e_minfo.as<uint32_t>();
   A.tmp_h = c->e_tmp_h.as<uint16_t>(); A.srt_h = c->e_srt_h.as<uint16_t>();
   A.tk_i = c->e_tk_i.as<uint32_t>(); A.tk_m = c->e_tk_m.as<uint32_t>(); A.tk_d = c->e_tk_d.as<uint32_t>();
   A.bcnt = c->e_bcnt.as<uint32_t>();
@@ -461,7 +462,7 @@ void zc_close(zc_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
-  for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_rank, &c->e_minfo, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
+  for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_minfo, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
                     &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
                     &c->e_bits, &c->e_lanes, &c->e_freq, &c->e_lanelen, &c->e_sinfo, &c->e_slab, &c->d_lit, &c->d_tok,
                     &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta})
@@ -588,6 +589,7 @@ int zc_get_shape(const zc_ctx* c, uint32_t block_log, int level, zc_shape* out) 
   out->fill_ring_log = s.ring_log;
   out->fill_warps = s.fill_warps;
   out->match_cap = s.cmp_cap;
+  out->match_tile = s.match_tile;
   return ZC_OK;
 }
 
@@ -597,13 +599,15 @@ int zc_set_shape(zc_ctx* c, uint32_t block_log, int level, const zc_shape* in) {
   const uint32_t w = in->fill_warps;
   if (in->fill_ring_log < zc::kMinFillRingLog || in->fill_ring_log > zc::kMaxFillRingLog ||
       (w != 1 && w != 2 && w != 4 && w != 8) || in->match_cap < 8 ||
-      in->match_cap > 32 || zc::fill_smem_bytes(in->fill_ring_log, w) > zc::kMaxFillSmem)
+      in->match_cap > 32 || zc::fill_smem_bytes(in->fill_ring_log, w) > zc::kMaxFillSmem ||
+      (in->match_tile != 256 && in->match_tile != 512 && in->match_tile != 1024))
     return fail(c, ZC_E_ARG, "launch shape out of range");
   ZC_CUDA(cudaSetDevice(c->device));
   Shape& s = c->shape[block_log - zc::kMinBlockLog][level_class(level)];
   s.ring_log = in->fill_ring_log;
   s.fill_warps = w;
   s.cmp_cap = in->match_cap;
+  s.match_tile = in->match_tile;
   drop_graphs(c);  // (captured launches carry the old shape)
   return ZC_OK;
 }
@@ -684,13 +688,16 @@ int zc_autotune(zc_ctx* c, const uint8_t* sample, size_t n, uint32_t block_log, 
     if (e != cudaSuccess) { r = cuda_fail(c, e, "autotune set-up"); break; }
     Shape best = saved;
     float best_ms = 1e30f;
-    for (uint32_t cap : {12u, 16u, 20u, 24u, 28u, 32u}) {
-      cur = best;
-      cur.cmp_cap = cap;
-      float ms;
-      if ((r = timed(encode, ms))) break;
-      if (ms < best_ms) { best_ms = ms; best.cmp_cap = cap; }
-    }
+    for (uint32_t cap : {12u, 16u, 24u, 32u})
+      for (uint32_t tile : {256u, 512u, 1024u}) {
+        if (r) break;
+        cur = best;
+        cur.cmp_cap = cap;
+        cur.match_tile = tile;
+        float ms;
+        if ((r = timed(encode, ms))) break;
+        if (ms < best_ms) { best_ms = ms; best.cmp_cap = cap; best.match_tile = tile; }
+      }
     if (r) break;
     cur = best;
     if ((r = encode())) break;  // (every cap writes the same payloads)

@@ -7,11 +7,13 @@
 //
 //   k_enc_sort     one CTA per block: stable two-pass LSD radix sort of the positions by hash
 //                  (8 + 8 bits; per-warp histograms, warp match_any ranks; no global atomics)
-//   k_enc_match    one thread per sorted position: scans its chain, comparing at most cmp_cap bytes;
-//                  a match that reaches cmp_cap is marked and finished only if the parse visits it
+//   k_enc_match    per sorted position (lanes take positions from a per-CTA counter): scans its chain,
+//                  comparing at most cmp_cap bytes; a match that reaches cmp_cap is marked and finished
+//                  only if the parse visits it
 //   k_enc_parse    one CTA per block: the greedy + lazy parse as a chain 0 -> next(0) -> ..., walked
 //                  per segment in parallel from the segment start, then re-walked from the true entry
-//                  until it meets the first walk (rounds until no segment exit moves)
+//                  until it meets the first walk (rounds until no segment exit moves); a warp's walks
+//                  step together and finish capped matches as a warp
 //   k_enc_streams  one warp per block: groups, recent offsets, tok / ext / sym / group streams, offset
 //                  bits (a warp-private bit window, no atomics on global memory), literals
 //   k_enc_rans     one CTA per (block, stream): histogram, 12-bit normalisation with the reference's
@@ -23,13 +25,13 @@
 
 namespace zc {
 
-// per-position match record: NONE; SAT | k (a candidate reached cmp_cap, the first of them k steps back
-// in the chain: finished on demand by the parse); or the exact (length - 4) << 20 | (distance - 1).
-// Lengths are <= 4096, so an exact record never has 0xFFF in its top 12 bits.
+// per-position match record: NONE; SAT | r (a candidate reached cmp_cap; r is the position's index in the
+// hash-sorted order, where its chain starts: finished on demand by the parse); or the exact
+// (length - 4) << 20 | (distance - 1).  Lengths are <= 4096, so an exact record never has 0xFFF in its
+// top 12 bits, and r < 2^20 - 3, so SAT | r is never NONE.
 constexpr uint32_t M_NONE = 0xFFFFFFFFu;
 constexpr uint32_t M_SAT = 0xFFF00000u;
 __device__ __forceinline__ bool m_is_sat(uint32_t v) { return (v >> 20) == 0xFFFu && v != M_NONE; }
-constexpr uint32_t kWin = 32;  // bytes of each sorted position kept in shared memory by the match pass
 __device__ __forceinline__ uint32_t m_pack(uint32_t m, uint32_t d) { return ((m - 4u) << 20) | (d - 1u); }
 __device__ __forceinline__ uint32_t m_len(uint32_t v) { return (v >> 20) + 4u; }
 __device__ __forceinline__ uint32_t m_dist(uint32_t v) { return (v & 0xFFFFFu) + 1u; }
@@ -172,6 +174,15 @@ __global__ void __launch_bounds__(1024) k_enc_sort(EncArgs A) {
 }
 
 // ---------------------------------------------------------------- 2. capped matches at every position
+// the first differing byte of two 16-byte windows (16 when equal)
+__device__ __forceinline__ uint32_t lcp16(const uint4& a0, const uint4& b0) {
+  uint32_t x;
+  if ((x = a0.x ^ b0.x)) return ((uint32_t)__ffs(x) - 1u) >> 3;
+  if ((x = a0.y ^ b0.y)) return 4 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  if ((x = a0.z ^ b0.z)) return 8 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  if ((x = a0.w ^ b0.w)) return 12 + (((uint32_t)__ffs(x) - 1u) >> 3);
+  return 16;
+}
 // the first differing byte of two 32-byte windows (32 when equal)
 __device__ __forceinline__ uint32_t lcp32(const uint4& a0, const uint4& a1, const uint4& b0, const uint4& b1) {
   uint32_t x;
@@ -186,28 +197,38 @@ __device__ __forceinline__ uint32_t lcp32(const uint4& a0, const uint4& a1, cons
   return 32;
 }
 
-// One CTA per 256 consecutive sorted positions of a block.  The entries it needs (its own and the
-// `depth` before them) are staged once in shared memory with the first 32 bytes at each position, so
-// a candidate costs a few shared loads and XORs instead of random global reads.  Dynamic shared memory:
-// (256 + depth) * (32 + 4 + 2) bytes.
+// One CTA of 256 threads per `tile` consecutive sorted positions of a block (tile = A.match_tile, a
+// multiple of 256).  The entries it needs (its own and the `depth` before them) are staged once in
+// shared memory with the first WB bytes at each position (WB = 16 or 32, at least the compare cap), so
+// a candidate costs a few shared loads and XORs instead of random global reads.  Chains differ in length, so lanes do not own fixed positions:
+// each lane takes the CTA's next unscanned position from a shared counter whenever its own is finished
+// (a warp claims positions for all its idle lanes at once), keeping warps full until the tile drains.
+// A candidate whose byte at the current best length differs from the position's cannot be longer and
+// is skipped after one shared byte load (the CPU parse's probe, src/codec2.h:62).
+// Dynamic shared memory: (tile + depth) * (WB + 4 + 2) bytes.
+template <uint32_t WB>
 __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
+  constexpr uint32_t NV = WB / 16;  // uint4s per window
   extern __shared__ uint4 sm[];
-  const uint32_t b = blockIdx.y, t = threadIdx.x;
-  const uint32_t r0 = blockIdx.x * 256;
+  __shared__ uint32_t next;
+  const uint32_t b = blockIdx.y, t = threadIdx.x, lane = lane_id();
+  const uint32_t tile = A.match_tile;
+  const uint32_t r0 = blockIdx.x * tile;
   const uint32_t n = A.in_len[b];
   if (r0 >= n) return;
   const uint32_t count = n >= 4 ? n - 3 : 0;
   const size_t so = (size_t)b * A.B;
   const uint32_t D = (uint32_t)A.depth;
-  const uint32_t cap_e = 256 + D;
-  uint4* wlo = sm;
-  uint4* whi = wlo + cap_e;
-  uint32_t* spos = reinterpret_cast<uint32_t*>(whi + cap_e);
+  const uint32_t cap_e = tile + D;
+  uint4* win = sm;  // entry i: bytes 16 v .. 16 v + 15 at win[NV i + v]
+  uint32_t* spos = reinterpret_cast<uint32_t*>(win + NV * cap_e);
   uint16_t* sh = reinterpret_cast<uint16_t*>(spos + cap_e);
-  const uint32_t e0 = r0 > D ? r0 - D : 0, e1 = min(r0 + 256, count);
+  const uint8_t* wb = reinterpret_cast<const uint8_t*>(win);
+  const uint32_t e0 = r0 > D ? r0 - D : 0, e1 = min(r0 + tile, count);
   const uint64_t base = A.in_off[b];
   const uint32_t* w32 = reinterpret_cast<const uint32_t*>(A.in);
   const uint64_t wend = (base + n + 3) >> 2;  // words at or past it are not read (they lie past the block)
+  if (t == 0) next = 0;
   for (uint32_t i = t; e0 + i < e1; i += 256) {
     const uint32_t r = e0 + i;
     const uint32_t p = A.srt_pos[so + r];
@@ -215,40 +236,87 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
     sh[i] = A.srt_h[so + r];
     const uint64_t a = base + p, wa = a >> 2;
     const uint32_t shf = (uint32_t)(a & 3u) * 8u;
-    uint32_t w[9];
+    uint32_t w[WB / 4 + 1];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) w[q] = wa + q < wend ? __ldg(w32 + wa + q) : 0u;
-    uint32_t v[8];
+    for (uint32_t q = 0; q <= WB / 4; ++q) w[q] = wa + q < wend ? __ldg(w32 + wa + q) : 0u;
+    uint32_t v[WB / 4];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = __funnelshift_r(w[q], w[q + 1], shf);
-    wlo[i] = make_uint4(v[0], v[1], v[2], v[3]);
-    whi[i] = make_uint4(v[4], v[5], v[6], v[7]);
+    for (uint32_t q = 0; q < WB / 4; ++q) v[q] = __funnelshift_r(w[q], w[q + 1], shf);
+#pragma unroll
+    for (uint32_t q = 0; q < NV; ++q) win[NV * i + q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
   }
+  // positions past the last hashed one (the block's final 3 bytes) have no match
+  for (uint32_t r = max(r0, count) + t; r < min(r0 + tile, n); r += 256) A.minfo[so + r] = M_NONE;
   __syncthreads();
-  const uint32_t r = r0 + t;
-  if (r >= count) { if (r < n) A.minfo[so + r] = M_NONE; return; }
-  const uint32_t li = r - e0;
-  const uint32_t p = spos[li], h = sh[li];
-  A.rank[so + p] = r;
-  const uint32_t lim = min(kMaxMatch, n - p), cap = min(min(A.cmp_cap, kWin), lim);
-  const uint4 p0 = wlo[li], p1 = whi[li];
-  uint32_t best = 0, bd = 0, kf = 0;
-  const uint32_t kmax = min(D, r);
-  for (uint32_t k = 1; k <= kmax; ++k) {
-    const uint32_t e = li - k;
-    if (sh[e] != h) break;
-    const uint32_t l = min(lcp32(wlo[e], whi[e], p0, p1), cap);
-    if (l > best) {
-      best = l;
-      bd = p - spos[e];
-      if (best == cap) { kf = k; break; }
+  const uint32_t tn = e1 > r0 ? e1 - r0 : 0;  // positions of this tile
+  // per-lane scan state: the position's entry li, its chain of kend earlier entries with the same hash
+  // (found by a binary search: the entries are sorted by hash), the candidate k reached so far, the
+  // best length, its distance, and the position's own byte at offset `best` (the probe)
+  uint32_t li = 0xFFFFFFFFu, p = 0, lim = 0, cap = 0, best = 0, bd = 0, k = 0, kend = 0, pb = 0;
+  uint4 p0 = make_uint4(0, 0, 0, 0), p1 = p0;
+  bool dry = false;  // the tile has no unclaimed positions left (warp-uniform)
+  for (;;) {
+    const bool idle = li == 0xFFFFFFFFu;
+    const unsigned want = __ballot_sync(kFull, idle);
+    if (want && !dry) {
+      const uint32_t leader = (uint32_t)__ffs(want) - 1u;
+      uint32_t got = 0;
+      if (lane == leader) got = atomicAdd(&next, (uint32_t)__popc(want));
+      got = __shfl_sync(kFull, got, leader);
+      if (got + (uint32_t)__popc(want) >= tn) dry = true;
+      if (idle) {
+        const uint32_t my = got + (uint32_t)__popc(want & ((1u << lane) - 1u));
+        if (my < tn) {
+          const uint32_t r = r0 + my;
+          li = r - e0;
+          p = spos[li];
+          const uint32_t h = sh[li];
+          lim = min(kMaxMatch, n - p);
+          cap = min(min(A.cmp_cap, WB), lim);
+          p0 = win[NV * li];
+          p1 = win[NV * li + NV - 1];
+          best = 0; bd = 0; k = 0; pb = 0;
+          uint32_t lo = li - min(D, r), hi = li;  // the first entry of [lo, li] with hash h
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sh[mid] < h) lo = mid + 1; else hi = mid;
+          }
+          kend = li - lo;
+        }
+      }
+    }
+    if (!__any_sync(kFull, li != 0xFFFFFFFFu)) break;
+    if (li == 0xFFFFFFFFu) continue;
+    // four candidates of this lane's chain: probes first, full compares for those that pass, in order
+    bool fin = false;
+    uint32_t pass = 0;
+#pragma unroll
+    for (uint32_t u = 0; u < 4; ++u) {
+      const uint32_t kk = k + 1 + u;
+      if (kk <= kend && (best == 0 || wb[WB * (li - kk) + best] == pb)) pass |= 1u << u;
+    }
+    while (pass) {
+      const uint32_t u = (uint32_t)__ffs(pass) - 1u;
+      pass &= pass - 1u;
+      const uint32_t kk = k + 1 + u, e = li - kk;
+      const uint32_t l = min(NV == 2 ? lcp32(win[2 * e], win[2 * e + 1], p0, p1) : lcp16(win[e], p0), cap);
+      if (l > best) {
+        best = l;
+        bd = p - spos[e];
+        if (best == cap) { fin = true; break; }
+        pb = wb[WB * li + best];
+      }
+    }
+    k += 4;
+    if (fin || k >= kend) {
+      uint32_t v;
+      if (best < 4) v = M_NONE;
+      else if (best == cap && cap < lim) v = M_SAT | (li + e0);
+      else v = m_pack(best, bd);
+      A.minfo[so + p] = v;
+      li = 0xFFFFFFFFu;
     }
   }
-  uint32_t v;
-  if (best < 4) v = M_NONE;
-  else if (best == cap && cap < lim) v = M_SAT | kf;
-  else v = m_pack(best, bd);
-  A.minfo[so + p] = v;
 }
 
 // ---------------------------------------------------------------- 3. the parse
@@ -257,59 +325,120 @@ struct ParseBlock {
   uint64_t base;
   uint32_t n, depth;
   uint32_t* minfo;
-  const uint32_t* rank;
   const uint32_t* spos;
   const uint16_t* sh;
 };
 
-// the exact match at p (finishing a capped one: the whole chain compared up to 4096 bytes)
-__device__ uint32_t exact_match(const ParseBlock& P, uint32_t p) {
-  const uint32_t v = P.minfo[p];
+// The exact match at x, all 32 lanes together (x the same in every lane).  A capped record names x's
+// index r in the hash-sorted order; its chain is the entries before r with the same hash, nearest first
+// (the order src/codec2.h:58-67 walks them).  Up to 32 candidates at a time: each
+// lane compares its candidate's first 32 bytes; those equal for 32 bytes (when the match may be longer)
+// are extended in chain order by the whole warp, 128 bytes a step.  The longest wins, the nearest on a
+// tie, and a match of the whole remaining length ends the walk, as in the CPU parse.  The exact record
+// replaces the capped one in minfo.
+__device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x) {
+  const uint32_t lane = lane_id();
+  const uint32_t v = P.minfo[x];
   if (!m_is_sat(v)) return v;
-  const uint32_t r = P.rank[p], h = P.sh[r];
-  const uint32_t lim = min(kMaxMatch, P.n - p);
-  const uint64_t ap = P.base + p;
-  uint32_t best = 0, bd = 0;
+  const uint32_t r = v & 0xFFFFFu, h = P.sh[r];
+  const uint32_t lim = min(kMaxMatch, P.n - x);
+  const uint32_t l32 = min(32u, lim);
   const uint32_t kmax = min(P.depth, r);
-  // candidates before the first that reached the cap are shorter than it: start there
-  for (uint32_t k = max(1u, v & 0xFFFFFu); k <= kmax; ++k) {
-    if (P.sh[r - k] != h) break;
-    const uint32_t j = P.spos[r - k];
-    const uint64_t aj = P.base + j;
-    const uint32_t probe = min(best, lim - 1);
-    if (best && __ldg(P.in + aj + probe) != __ldg(P.in + ap + probe)) continue;
-    const uint32_t l = lcp(P.in, aj, ap, lim);
-    if (l > best) {
-      best = l;
-      bd = p - j;
-      if (best == lim) break;
+  const uint64_t ax = P.base + x;
+  uint32_t best = 0, bd = 0;
+  bool stop = false;
+  for (uint32_t kb = 1; kb <= kmax && !stop; kb += 32) {
+    const uint32_t k = kb + lane;
+    const bool in_chain = k <= kmax && P.sh[r - k] == h;
+    const unsigned chain = __ballot_sync(kFull, in_chain);
+    const unsigned live = ~chain ? chain & ((1u << __ffs(~chain) - 1) - 1u) : chain;  // up to the first break
+    if (live != chain || chain != kFull) stop = true;  // the chain ends in this chunk
+    const bool on = (live >> lane) & 1u;
+    const uint32_t j = on ? P.spos[r - k] : 0u;
+    const uint32_t l = on ? lcp(P.in, P.base + j, ax, l32) : 0u;
+    // candidates shorter than 32 bytes (or the whole remaining length): the longest, nearest on a tie
+    uint32_t key = on ? (l << 8) | (31u - lane) : 0u;  // (l <= 32, lanes in chain order)
+    key = __reduce_max_sync(kFull, key);
+    const uint32_t cl = key >> 8, cw = 31u - (key & 0xFFu);
+    const uint32_t jw = __shfl_sync(kFull, j, cw);
+    if (cl > best) { best = cl; bd = x - jw; }
+    if (best == lim) break;
+    // candidates equal for 32 bytes: extended in chain order
+    unsigned ext = __ballot_sync(kFull, on && l == 32u && lim > 32u);
+    while (ext) {
+      const uint32_t c = (uint32_t)__ffs(ext) - 1u;
+      ext &= ext - 1u;
+      const uint32_t jc = __shfl_sync(kFull, j, c);
+      const uint64_t aj = P.base + jc;
+      if (best > 32 && __ldg(P.in + aj + min(best, lim - 1)) != __ldg(P.in + ax + min(best, lim - 1))) continue;
+      uint32_t len = lim;
+      for (uint32_t o = 32; o < lim; o += 128) {
+        const uint32_t q = o + 4 * lane;
+        uint32_t diff = 0;
+        if (q < lim) diff = load4(P.in, aj + q) ^ load4(P.in, ax + q);
+        const uint32_t nb = q < lim ? (diff ? ((uint32_t)__ffs(diff) - 1u) >> 3 : 4u) : 0u;
+        const bool miss = q < lim && (nb < 4u || q + 4 > lim);
+        const unsigned mm = __ballot_sync(kFull, miss);
+        if (mm) {
+          const uint32_t f = (uint32_t)__ffs(mm) - 1u;
+          const uint32_t qf = o + 4 * f, nf = __shfl_sync(kFull, nb, f);
+          len = min(qf + nf, lim);
+          break;
+        }
+      }
+      if (len > best) {
+        best = len;
+        bd = x - jc;
+        if (best == lim) { stop = true; break; }
+      }
     }
   }
   const uint32_t e = m_pack(best, bd);
-  P.minfo[p] = e;  // (every thread that finishes it writes the same value)
+  __syncwarp();
+  if (lane == 0) P.minfo[x] = e;
+  __syncwarp();
   return e;
 }
 
-// one step of the CPU parse from position p (src/codec2.h:69-80): returns the next position; a token,
-// when the step emits one, in (ti, tm, td)
-__device__ __forceinline__ uint32_t parse_step(const ParseBlock& P, uint32_t p, bool& tok, uint32_t& ti, uint32_t& tm,
-                                               uint32_t& td) {
-  const uint32_t v = exact_match(P, p);
-  if (v == M_NONE) { tok = false; return p + 1; }
+// One step of the CPU parse (src/codec2.h:69-80) for every lane with `act` (all 32 lanes call it):
+// returns the next position (p itself when !act); the token, when the step emits one, in (ti, tm, td).
+// Capped records at p or p + 1 are finished first, one at a time, by the whole warp.
+__device__ __forceinline__ uint32_t warp_step(const ParseBlock& P, uint32_t p, bool act, bool& tok, uint32_t& ti,
+                                              uint32_t& tm, uint32_t& td) {
+  uint32_t v = act ? P.minfo[p] : M_NONE;
+  const bool lz = act && v != M_NONE && p + 1 < P.n;
+  uint32_t v2 = lz ? P.minfo[p + 1] : M_NONE;
+  unsigned s1 = __ballot_sync(kFull, act && m_is_sat(v));
+  while (s1) {
+    const uint32_t L = (uint32_t)__ffs(s1) - 1u;
+    s1 &= s1 - 1u;
+    const uint32_t e = coop_exact(P, __shfl_sync(kFull, p, L));
+    if (lane_id() == L) v = e;
+  }
+  unsigned s2 = __ballot_sync(kFull, lz && m_is_sat(v2));
+  while (s2) {
+    const uint32_t L = (uint32_t)__ffs(s2) - 1u;
+    s2 &= s2 - 1u;
+    const uint32_t e = coop_exact(P, __shfl_sync(kFull, p, L) + 1u);
+    if (lane_id() == L) v2 = e;
+  }
+  tok = false;
+  if (!act) return p;
+  if (v == M_NONE) return p + 1;
   uint32_t m = m_len(v), d = m_dist(v), at = p;
-  if (p + 1 < P.n && P.minfo[p + 1] != M_NONE) {
-    const uint32_t v2 = exact_match(P, p + 1);
+  if (lz && v2 != M_NONE) {
     const uint32_t m2 = m_len(v2), d2 = m_dist(v2);
     if ((int)(8 * m2) - (int)bitlen(d2) - 8 > (int)(8 * m) - (int)bitlen(d)) { at = p + 1; m = m2; d = d2; }
   }
   tok = true; ti = at; tm = m; td = d;
   return at + m;
 }
-__device__ __forceinline__ uint32_t parse_next(const ParseBlock& P, uint32_t p) {
-  bool t; uint32_t a, c, d;
-  return parse_step(P, p, t, a, c, d);
-}
 
+// One CTA per block, 256 segments of the block, a lane each.  The parse is a chain 0 -> next(0) -> ...;
+// round 0 walks every segment from its own start; each later round re-walks a segment from where the
+// chain before it leaves, until that walk meets the previous one (a two-pointer merge), and rounds end
+// when no segment's exit moves.  Then every segment counts and writes its tokens.  Each warp's 32 walks
+// step together (warp_step), so capped matches are finished by whole warps.
 __global__ void __launch_bounds__(256) k_enc_parse(EncArgs A) {
   const uint32_t b = blockIdx.x, q = threadIdx.x;
   const uint32_t n = A.in_len[b];
@@ -317,13 +446,14 @@ __global__ void __launch_bounds__(256) k_enc_parse(EncArgs A) {
   __shared__ uint32_t ent[256], ex[256], wsum[8];
   ParseBlock P;
   P.in = A.in; P.base = A.in_off[b]; P.n = n; P.depth = (uint32_t)A.depth;
-  P.minfo = A.minfo + so; P.rank = A.rank + so; P.spos = A.srt_pos + so; P.sh = A.srt_h + so;
+  P.minfo = A.minfo + so; P.spos = A.srt_pos + so; P.sh = A.srt_h + so;
   const uint32_t S = max(1u, (n + 255) / 256);
   const uint32_t s = min(q * S, n), e = min(s + S, n);
+  bool t; uint32_t ta, tc, td;
   // round 0: every segment walked from its own start
   {
     uint32_t p = s;
-    while (p < e) p = parse_next(P, p);
+    while (__any_sync(kFull, p < e)) p = warp_step(P, p, p < e, t, ta, tc, td);
     ent[q] = s;
     ex[q] = s < e ? p : s;
   }
@@ -334,22 +464,27 @@ __global__ void __launch_bounds__(256) k_enc_parse(EncArgs A) {
     __syncthreads();
     bool changed = false;
     const uint32_t old_ent = ent[q], old_ex = ex[q];
+    // mode 0: settled; 1: walk a until it leaves the segment; 2: advance the lower of a (new walk) and
+    // c (old walk) until they meet or both leave
+    int mode = 0;
+    uint32_t a = want, c = old_ent, nx = old_ex;
     if (want != old_ent) {
-      uint32_t nx;
-      if (want >= e) {
-        nx = want;
-      } else if (old_ent >= e) {
-        uint32_t a = want;
-        while (a < e) a = parse_next(P, a);
-        nx = a;
-      } else {
-        uint32_t a = want, c = old_ent;
-        for (;;) {
-          if (a == c) { nx = old_ex; break; }
-          if (a >= e && c >= e) { nx = a; break; }
-          if (a < c) a = parse_next(P, a); else c = parse_next(P, c);
-        }
+      if (want >= e) nx = want;
+      else mode = old_ent >= e ? 1 : 2;
+    }
+    while (__any_sync(kFull, mode != 0)) {
+      const bool adv_a = mode == 1 || (mode == 2 && a < c);
+      const uint32_t y = warp_step(P, adv_a ? a : c, mode != 0, t, ta, tc, td);
+      if (mode == 1) {
+        a = y;
+        if (a >= e) { nx = a; mode = 0; }
+      } else if (mode == 2) {
+        if (adv_a) a = y; else c = y;
+        if (a == c) { nx = old_ex; mode = 0; }
+        else if (a >= e && c >= e) { nx = a; mode = 0; }
       }
+    }
+    if (want != old_ent) {
       ent[q] = want;
       if (nx != old_ex) { ex[q] = nx; changed = true; }
     }
@@ -358,9 +493,8 @@ __global__ void __launch_bounds__(256) k_enc_parse(EncArgs A) {
   // tokens: count per segment, offsets, then write
   const uint32_t from = ent[q];
   uint32_t cnt = 0;
-  for (uint32_t p = from; p < e;) {
-    bool t; uint32_t a, c, d;
-    p = parse_step(P, p, t, a, c, d);
+  for (uint32_t p = from; __any_sync(kFull, p < e);) {
+    p = warp_step(P, p, p < e, t, ta, tc, td);
     cnt += t;
   }
   const uint32_t incl = warp_incl_scan(cnt);
@@ -369,10 +503,9 @@ __global__ void __launch_bounds__(256) k_enc_parse(EncArgs A) {
   uint32_t off = incl - cnt;
   for (uint32_t k = 0; k < (q >> 5); ++k) off += wsum[k];
   const size_t to = (size_t)b * tok_cap(A.B);
-  for (uint32_t p = from; p < e;) {
-    bool t; uint32_t a, c, d;
-    p = parse_step(P, p, t, a, c, d);
-    if (t) { A.tk_i[to + off] = a; A.tk_m[to + off] = c; A.tk_d[to + off] = d; ++off; }
+  for (uint32_t p = from; __any_sync(kFull, p < e);) {
+    p = warp_step(P, p, p < e, t, ta, tc, td);
+    if (t) { A.tk_i[to + off] = ta; A.tk_m[to + off] = tc; A.tk_d[to + off] = td; ++off; }
   }
   if (q == 255) A.bcnt[b * 8 + 0] = off;
 }
@@ -732,8 +865,16 @@ __global__ void __launch_bounds__(256) k_enc_emit(EncArgs A) {
   for (uint32_t k = i + threadIdx.x; k < len; k += blockDim.x) d[k] = s[k];
 }
 
+size_t match_smem_bytes(uint32_t tile, uint32_t depth, uint32_t wb) { return (size_t)(tile + depth) * (wb + 4 + 2); }
+
 cudaError_t prepare_kernels() {  // with the device current, once per context
   cudaError_t e = cudaFuncSetAttribute(k_enc_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_enc_match<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)match_smem_bytes(kMaxMatchTile, 256, 32));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_enc_match<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)match_smem_bytes(kMaxMatchTile, 256, 16));
   return e == cudaSuccess ? prepare_fill() : e;
 }
 
@@ -744,8 +885,9 @@ void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Sta
   k_enc_sort<<<A.nb, 1024, kSortSmem, st>>>(A);
   S.end(st);
   S.begin("k_enc_match", st);
-  const size_t msm = (size_t)(256 + A.depth) * (2 * sizeof(uint4) + 4 + 2);
-  k_enc_match<<<dim3((A.B + 255) / 256, A.nb), 256, msm, st>>>(A);
+  const dim3 mg((A.B + A.match_tile - 1) / A.match_tile, A.nb);
+  if (A.cmp_cap <= 16) k_enc_match<16><<<mg, 256, match_smem_bytes(A.match_tile, (uint32_t)A.depth, 16), st>>>(A);
+  else k_enc_match<32><<<mg, 256, match_smem_bytes(A.match_tile, (uint32_t)A.depth, 32), st>>>(A);
   S.end(st);
   S.begin("k_enc_parse", st);
   k_enc_parse<<<A.nb, 256, 0, st>>>(A);

@@ -72,8 +72,9 @@ struct EncArgs {
   uint32_t nb, B, block_log;
   int depth;                  // hash chain steps (8 / 32 / 256)
   uint32_t cmp_cap;           // bytes the all-position match pass compares before deferring to the parse
+  uint32_t match_tile;        // sorted positions per match CTA: 256, 512 or 1024
   // scratch, per block slot (capacity B positions)
-  uint32_t *tmp_pos, *srt_pos, *rank, *minfo;
+  uint32_t *tmp_pos, *srt_pos, *minfo;
   uint16_t *tmp_h, *srt_h;
   uint32_t *tk_i, *tk_m, *tk_d;   // tokens, tok_cap(B) per block
   uint32_t* bcnt;                 // per block [8]: nt, nl, ne, nob, ng, payload size, method
@@ -110,6 +111,8 @@ __host__ __device__ inline uint64_t lanes_per_block(uint32_t B) { return lane_ba
 __host__ __device__ inline uint32_t bits_cap(uint32_t B) { return 5 * B / 8 + 64; }
 
 void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Stages& S);
+constexpr uint32_t kMaxMatchTile = 1024;
+size_t match_smem_bytes(uint32_t tile, uint32_t depth, uint32_t window_bytes);
 cudaError_t prepare_kernels();
 cudaError_t prepare_fill();  // per-kernel attributes (the sort's shared memory), the device current
 
