@@ -5,8 +5,9 @@
 // 4-byte hash (16 bits) equals i's, the longest match kept (the nearest on a tie), one lazy step.  A
 // chain is exactly the run of i's predecessors in a stable sort of the positions by hash, so:
 //
-//   k_enc_sort     one CTA per block: stable two-pass LSD radix sort of the positions by hash
-//                  (8 + 8 bits; per-warp histograms, warp match_any ranks; no global atomics)
+//   k_sort_*       stable two-pass LSD radix sort of each block's positions by hash (8 + 8 bits), a
+//                  CTA per 4096-position tile: digit counts, per-block scan, ranked scatter (warp
+//                  match_any ranks, the tile reordered in shared memory, digit runs written together)
 //   k_enc_match    per sorted position (lanes take positions from a per-CTA counter): scans its chain,
 //                  comparing at most cmp_cap bytes; a match that reaches cmp_cap is marked and finished
 //                  only if the parse visits it
@@ -61,115 +62,143 @@ __device__ __forceinline__ uint32_t lcp(const uint8_t* base, uint64_t a, uint64_
 }
 
 // ---------------------------------------------------------------- 1. stable sort by hash
-// Two stable LSD passes over the 16-bit hash (low byte, then high byte).  Each pass walks the block in
-// tiles of 4096 positions: a tile is ranked per digit (per-warp counts, __match_any_sync ranks), reordered
-// by digit in shared memory, and written out so that each digit's run is one contiguous global write.
-// Both passes' digit histograms come from one sweep.  Dynamic shared memory: kSortSmem bytes.
-constexpr uint32_t kSortTile = 4096, kSortPer = kSortTile / 1024;  // positions per tile, per thread
-constexpr size_t kSortSmem = 32 * 256 * 4 + kSortTile * 6 + 5 * 256 * 4;
+// Two stable LSD passes over the 16-bit hash (low byte, then high byte), each as three kernels over
+// tiles of 4096 positions, every tile its own CTA: k_sort_count (the tile's digit counts), k_sort_scan
+// (per block: each tile's start for each digit, digit-major), k_sort_scatter (ranks the tile's entries
+// per digit in order with warp match_any, reorders the tile by digit in shared memory, and writes each
+// digit's run to its place).  Pass 0 reads positions in order and hashes them; pass 1 reads pass 0's
+// output.  The counts array holds tiles_per_block(B) * 256 words per block.
+constexpr uint32_t kSortTile = 4096, kSortThreads = 512, kSortPer = kSortTile / kSortThreads;
 
-__global__ void __launch_bounds__(1024) k_enc_sort(EncArgs A) {
-  extern __shared__ uint32_t ss[];
-  uint32_t (*cw)[256] = reinterpret_cast<uint32_t (*)[256]>(ss);  // per-warp digit counts of a tile
-  uint32_t* st_pos = ss + 32 * 256;                                // the tile reordered by digit
-  uint16_t* st_h = reinterpret_cast<uint16_t*>(st_pos + kSortTile);
-  uint32_t* hist = reinterpret_cast<uint32_t*>(st_h + kSortTile);  // [2][256] block histograms
-  uint32_t* base = hist + 512;                                     // digit start in the block
-  uint32_t* tds = base + 256;                                      // digit start in the tile
-  uint32_t* tot = tds + 256;                                       // digit count in the tile
-  const uint32_t b = blockIdx.x;
-  const uint32_t n = A.in_len[b];
-  const uint32_t count = n >= 4 ? n - 3 : 0;  // positions with 4 bytes left (src/codec2.h:52, 58)
-  if (!count) return;
-  const uint32_t tid = threadIdx.x, w = tid >> 5, lane = tid & 31u;
-  const uint64_t in0 = A.in_off[b];
-  const size_t so = (size_t)b * A.B;
-  uint32_t* tpos = A.tmp_pos + so;
-  uint16_t* th = A.tmp_h + so;
-  uint32_t* spos = A.srt_pos + so;
-  uint16_t* sh = A.srt_h + so;
-  for (uint32_t i = tid; i < 512; i += 1024) hist[i] = 0;
+__device__ __forceinline__ uint32_t sort_tiles(uint32_t B) { return (B + kSortTile - 1) / kSortTile; }
+
+template <int PASS>
+__device__ __forceinline__ void sort_load(const EncArgs& A, uint32_t b, uint32_t i, uint32_t& p, uint32_t& h) {
+  if (PASS == 0) {
+    p = i;
+    h = hash16(A.in, A.in_off[b] + i);
+  } else {
+    const size_t so = (size_t)b * A.B;
+    p = A.tmp_pos[so + i];
+    h = A.tmp_h[so + i];
+  }
+}
+template <int PASS>
+__device__ __forceinline__ uint32_t sort_digit(uint32_t h) { return PASS == 0 ? (h & 0xFFu) : (h >> 8); }
+
+template <int PASS>
+__global__ void __launch_bounds__(256) k_sort_count(EncArgs A) {
+  const uint32_t b = blockIdx.y, t = blockIdx.x, tid = threadIdx.x, lane = lane_id();
+  __shared__ uint32_t hist[256];
+  const uint32_t n = A.in_len[b], count = n >= 4 ? n - 3 : 0;
+  const uint32_t i0 = t * kSortTile, i1 = min(i0 + kSortTile, count);
+  hist[tid] = 0;
   __syncthreads();
-  for (uint32_t i = tid; i < count; i += 1024) {
-    const uint32_t h = hash16(A.in, in0 + i);
-    atomicAdd(&hist[h & 0xFFu], 1u);
-    atomicAdd(&hist[256 + (h >> 8)], 1u);
+  for (uint32_t base = i0; base < i1; base += 256) {
+    const uint32_t i = base + tid;
+    const bool on = i < i1;
+    uint32_t p = 0, h = 0;
+    if (on) sort_load<PASS>(A, b, i, p, h);
+    const uint32_t d = sort_digit<PASS>(h);
+    const unsigned act = __ballot_sync(kFull, on);
+    if (on) {
+      const unsigned peers = __match_any_sync(act, d);
+      if (lane == (uint32_t)__ffs(peers) - 1u) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+    }
   }
   __syncthreads();
-  for (int pass = 0; pass < 2; ++pass) {
-    if (w == 0) {  // digit starts: exclusive scan of this pass's histogram
-      uint32_t v[8], sum = 0;
+  A.scnt[((size_t)b * sort_tiles(A.B) + t) * 256 + tid] = hist[tid];
+}
+
+// per block: counts -> each tile's start per digit (digit-major order over the block's tiles)
+__global__ void __launch_bounds__(256) k_sort_scan(EncArgs A) {
+  const uint32_t b = blockIdx.x, d = threadIdx.x, lane = lane_id(), w = d >> 5;
+  __shared__ uint32_t ws[8];
+  const uint32_t T = sort_tiles(A.B);
+  uint32_t* c = A.scnt + (size_t)b * T * 256;
+  uint32_t run = 0;
+  for (uint32_t t = 0; t < T; ++t) {
+    const uint32_t v = c[t * 256 + d];
+    c[t * 256 + d] = run;
+    run += v;
+  }
+  const uint32_t inc = warp_incl_scan(run);
+  if (lane == 31) ws[w] = inc;
+  __syncthreads();
+  uint32_t base = inc - run;
+  for (uint32_t k = 0; k < w; ++k) base += ws[k];
+  for (uint32_t t = 0; t < T; ++t) c[t * 256 + d] += base;
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(EncArgs A) {
+  constexpr uint32_t NW = kSortThreads / 32;
+  __shared__ uint32_t cw[NW][256];  // per-warp digit counts, then the warp's start within the digit
+  __shared__ uint32_t st_pos[kSortTile];
+  __shared__ uint16_t st_h[kSortTile];
+  __shared__ uint32_t tds[256], dst[256], ws[8];
+  const uint32_t b = blockIdx.y, t = blockIdx.x, tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
+  const uint32_t n = A.in_len[b], count = n >= 4 ? n - 3 : 0;
+  const uint32_t i0 = t * kSortTile;
+  if (i0 >= count) return;
+  const uint32_t tn = min(kSortTile, count - i0);
+  const size_t so = (size_t)b * A.B;
+  for (uint32_t k = tid; k < NW * 256; k += kSortThreads) (&cw[0][0])[k] = 0;
+  if (tid < 256) dst[tid] = A.scnt[((size_t)b * sort_tiles(A.B) + t) * 256 + tid];
+  __syncthreads();
+  // ranks: warp w holds the tile's entries [kSortPer * 32 w, kSortPer * 32 (w + 1)), 32 per round, in order
+  uint32_t kp[kSortPer], kh[kSortPer], kr[kSortPer];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) { v[k] = hist[pass * 256 + lane * 8 + k]; sum += v[k]; }
-      uint32_t ex = warp_incl_scan(sum) - sum;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) { base[lane * 8 + k] = ex; ex += v[k]; }
+  for (uint32_t j = 0; j < kSortPer; ++j) {
+    const uint32_t li = w * (32 * kSortPer) + j * 32 + lane;
+    const bool on = li < tn;
+    uint32_t p = 0, h = 0;
+    if (on) sort_load<PASS>(A, b, i0 + li, p, h);
+    const uint32_t d = sort_digit<PASS>(h);
+    const unsigned act = __ballot_sync(kFull, on);
+    uint32_t rk = 0xFFFFFFFFu;
+    if (on) {
+      const unsigned peers = __match_any_sync(act, d);
+      const uint32_t c = cw[w][d];
+      rk = c + __popc(peers & ((1u << lane) - 1u));
+      __syncwarp(act);
+      if ((peers & ((1u << lane) - 1u)) == 0) cw[w][d] = c + __popc(peers);
     }
-    for (uint32_t t0 = 0; t0 < count; t0 += kSortTile) {
-      for (uint32_t i = tid; i < 32 * 256; i += 1024) (&cw[0][0])[i] = 0;
-      __syncthreads();
-      // rank: warp w holds tile elements [128 w, 128 w + 128), 32 per round, in order
-      uint32_t kp[kSortPer], kh[kSortPer], kr[kSortPer];
+    __syncwarp();
+    kp[j] = p; kh[j] = h; kr[j] = rk;
+  }
+  __syncthreads();
+  if (tid < 256) {  // per digit: the warps' starts within it, and the tile's count
+    uint32_t run = 0;
 #pragma unroll
-      for (uint32_t j = 0; j < kSortPer; ++j) {
-        const uint32_t i = t0 + w * (32 * kSortPer) + j * 32 + lane;
-        const bool on = i < count;
-        uint32_t p = 0, h = 0;
-        if (on) {
-          if (pass == 0) { p = i; h = hash16(A.in, in0 + i); }
-          else { p = tpos[i]; h = th[i]; }
-        }
-        const uint32_t d = pass == 0 ? (h & 0xFFu) : (h >> 8);
-        const unsigned act = __ballot_sync(kFull, on);
-        uint32_t rk = 0;
-        if (on) {
-          const unsigned peers = __match_any_sync(act, d);
-          const uint32_t c = cw[w][d];
-          rk = c + __popc(peers & ((1u << lane) - 1u));
-          __syncwarp(act);
-          if ((peers & ((1u << lane) - 1u)) == 0) cw[w][d] = c + __popc(peers);
-        }
-        __syncwarp();
-        kp[j] = p; kh[j] = h; kr[j] = on ? rk : 0xFFFFFFFFu;
-      }
-      __syncthreads();
-      if (tid < 256) {  // per digit: counts of the warps before, the tile's count
-        uint32_t run = 0;
-        for (uint32_t k = 0; k < 32; ++k) { const uint32_t c = cw[k][tid]; cw[k][tid] = run; run += c; }
-        tot[tid] = run;
-      }
-      __syncthreads();
-      if (w == 0) {
-        uint32_t v[8], sum = 0;
+    for (uint32_t k = 0; k < NW; ++k) { const uint32_t c = cw[k][tid]; cw[k][tid] = run; run += c; }
+    const uint32_t inc = warp_incl_scan(run);
+    if (lane == 31) ws[w] = inc;
+    tds[tid] = inc - run;  // (the warp's part; the warps before are added below)
+  }
+  __syncthreads();
+  if (tid < 256) {
+    uint32_t add = 0;
+    for (uint32_t k = 0; k < w; ++k) add += ws[k];
+    tds[tid] += add;
+  }
+  __syncthreads();
 #pragma unroll
-        for (int k = 0; k < 8; ++k) { v[k] = tot[lane * 8 + k]; sum += v[k]; }
-        uint32_t ex = warp_incl_scan(sum) - sum;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) { tds[lane * 8 + k] = ex; ex += v[k]; }
-      }
-      __syncthreads();
-#pragma unroll
-      for (uint32_t j = 0; j < kSortPer; ++j) {
-        if (kr[j] == 0xFFFFFFFFu) continue;
-        const uint32_t d = pass == 0 ? (kh[j] & 0xFFu) : (kh[j] >> 8);
-        const uint32_t at = tds[d] + cw[w][d] + kr[j];
-        st_pos[at] = kp[j];
-        st_h[at] = (uint16_t)kh[j];
-      }
-      __syncthreads();
-      const uint32_t tn = min(kSortTile, count - t0);
-      for (uint32_t i = tid; i < tn; i += 1024) {
-        const uint32_t h = st_h[i];
-        const uint32_t d = pass == 0 ? (h & 0xFFu) : (h >> 8);
-        const uint32_t dest = base[d] + (i - tds[d]);
-        if (pass == 0) { tpos[dest] = st_pos[i]; th[dest] = (uint16_t)h; }
-        else { spos[dest] = st_pos[i]; sh[dest] = (uint16_t)h; }
-      }
-      __syncthreads();
-      if (tid < 256) base[tid] += tot[tid];
-      __syncthreads();
-    }
-    __syncthreads();
+  for (uint32_t j = 0; j < kSortPer; ++j) {
+    if (kr[j] == 0xFFFFFFFFu) continue;
+    const uint32_t d = sort_digit<PASS>(kh[j]);
+    const uint32_t at = tds[d] + cw[w][d] + kr[j];
+    st_pos[at] = kp[j];
+    st_h[at] = (uint16_t)kh[j];
+  }
+  __syncthreads();
+  uint32_t* op = PASS == 0 ? A.tmp_pos : A.srt_pos;
+  uint16_t* oh = PASS == 0 ? A.tmp_h : A.srt_h;
+  for (uint32_t i = tid; i < tn; i += kSortThreads) {
+    const uint32_t h = st_h[i], d = sort_digit<PASS>(h);
+    const size_t dest = so + dst[d] + (i - tds[d]);
+    op[dest] = st_pos[i];
+    oh[dest] = (uint16_t)h;
   }
 }
 
@@ -868,9 +897,7 @@ __global__ void __launch_bounds__(256) k_enc_emit(EncArgs A) {
 size_t match_smem_bytes(uint32_t tile, uint32_t depth, uint32_t wb) { return (size_t)(tile + depth) * (wb + 4 + 2); }
 
 cudaError_t prepare_kernels() {  // with the device current, once per context
-  cudaError_t e = cudaFuncSetAttribute(k_enc_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSortSmem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_enc_match<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_enc_match<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)match_smem_bytes(kMaxMatchTile, 256, 32));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_enc_match<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -881,8 +908,24 @@ cudaError_t prepare_kernels() {  // with the device current, once per context
 void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Stages& S) {
   if (!A.nb) return;
   launch_crc(crc_in, st, S, "k_crc_in");
-  S.begin("k_enc_sort", st);
-  k_enc_sort<<<A.nb, 1024, kSortSmem, st>>>(A);
+  const dim3 sg((A.B + kSortTile - 1) / kSortTile, A.nb);
+  S.begin("k_sort_count", st);
+  k_sort_count<0><<<sg, 256, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_sort_scan", st);
+  k_sort_scan<<<A.nb, 256, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_sort_scatter", st);
+  k_sort_scatter<0><<<sg, kSortThreads, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_sort_count", st);
+  k_sort_count<1><<<sg, 256, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_sort_scan", st);
+  k_sort_scan<<<A.nb, 256, 0, st>>>(A);
+  S.end(st);
+  S.begin("k_sort_scatter", st);
+  k_sort_scatter<1><<<sg, kSortThreads, 0, st>>>(A);
   S.end(st);
   S.begin("k_enc_match", st);
   const dim3 mg((A.B + A.match_tile - 1) / A.match_tile, A.nb);

@@ -75,6 +75,7 @@ struct EncArgs {
   uint32_t match_tile;        // sorted positions per match CTA: 256, 512 or 1024
   // scratch, per block slot (capacity B positions)
   uint32_t *tmp_pos, *srt_pos, *minfo;
+  uint32_t* scnt;                 // sort: per block ceil(B / 4096) * 256 tile digit counts / starts
   uint16_t *tmp_h, *srt_h;
   uint32_t *tk_i, *tk_m, *tk_d;   // tokens, tok_cap(B) per block
   uint32_t* bcnt;                 // per block [8]: nt, nl, ne, nob, ng, payload size, method
