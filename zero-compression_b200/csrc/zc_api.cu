@@ -131,7 +131,7 @@ struct zc_ctx {
   zc::CrcTables* d_crct = nullptr;
   // encoder scratch for enc_nb blocks of 2^enc_bl bytes
   uint32_t enc_nb = 0, enc_bl = 0;
-  DevBuf e_tmp_pos, e_srt_pos, e_minfo, e_scnt, e_tmp_h, e_srt_h, e_tk_i, e_tk_m, e_tk_d, e_bcnt, e_lit, e_tok,
+  DevBuf e_tmp_pos, e_srt_pos, e_minfo, e_scnt, e_tk_seg, e_tmp_h, e_srt_h, e_tk_i, e_tk_m, e_tk_d, e_bcnt, e_lit, e_tok,
       e_ext, e_sym, e_grp, e_bits, e_lanes, e_freq, e_lanelen, e_sinfo, e_slab;
   // decoder scratch for dec_nb blocks of 2^dec_bl bytes
   uint32_t dec_nb = 0, dec_bl = 0;
@@ -196,6 +196,7 @@ int ensure_enc(zc_ctx* c, uint32_t nb, uint32_t block_log) {
   ZC_CUDA(grow(c->e_srt_pos, N * 4));
   ZC_CUDA(grow(c->e_minfo, N * 4));
   ZC_CUDA(grow(c->e_scnt, (size_t)nb * ((B + 4095) / 4096) * 256 * 4));
+  ZC_CUDA(grow(c->e_tk_seg, (size_t)nb * 3 * zc::seg_tok_cap((uint32_t)B) * 4));
   ZC_CUDA(grow(c->e_tmp_h, N * 2));
   ZC_CUDA(grow(c->e_srt_h, N * 2));
   ZC_CUDA(grow(c->e_tk_i, nb * TC * 4));
@@ -270,6 +271,7 @@ int encode_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_off, const u
   A.match_tile = sh.match_tile;
   A.tmp_pos = c->e_tmp_pos.as<uint32_t>(); A.srt_pos = c->e_srt_pos.as<uint32_t>();
   A.minfo = c->e_minfo.as<uint32_t>(); A.scnt = c->e_scnt.as<uint32_t>();
+  A.tk_seg = c->e_tk_seg.as<uint32_t>();
   A.tmp_h = c->e_tmp_h.as<uint16_t>(); A.srt_h = c->e_srt_h.as<uint16_t>();
   A.tk_i = c->e_tk_i.as<uint32_t>(); A.tk_m = c->e_tk_m.as<uint32_t>(); A.tk_d = c->e_tk_d.as<uint32_t>();
   A.bcnt = c->e_bcnt.as<uint32_t>();
@@ -463,7 +465,7 @@ void zc_close(zc_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
-  for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_minfo, &c->e_scnt, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
+  for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_minfo, &c->e_scnt, &c->e_tk_seg, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
                     &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
                     &c->e_bits, &c->e_lanes, &c->e_freq, &c->e_lanelen, &c->e_sinfo, &c->e_slab, &c->d_lit, &c->d_tok,
                     &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta})

@@ -86,28 +86,51 @@ __device__ __forceinline__ void sort_load(const EncArgs& A, uint32_t b, uint32_t
 template <int PASS>
 __device__ __forceinline__ uint32_t sort_digit(uint32_t h) { return PASS == 0 ? (h & 0xFFu) : (h >> 8); }
 
+// each thread counts 16 consecutive entries of the tile: pass 0 hashes them from three aligned 16-byte
+// loads of the input (the 19 bytes it needs, inside the input's readable slack), pass 1 reads their
+// 16 hashes as two 16-byte loads; per-warp histograms in shared memory, summed at the end
 template <int PASS>
 __global__ void __launch_bounds__(256) k_sort_count(EncArgs A) {
-  const uint32_t b = blockIdx.y, t = blockIdx.x, tid = threadIdx.x, lane = lane_id();
-  __shared__ uint32_t hist[256];
+  const uint32_t b = blockIdx.y, t = blockIdx.x, tid = threadIdx.x, w = tid >> 5;
+  __shared__ uint32_t hist[8][256];
   const uint32_t n = A.in_len[b], count = n >= 4 ? n - 3 : 0;
   const uint32_t i0 = t * kSortTile, i1 = min(i0 + kSortTile, count);
-  hist[tid] = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) hist[k][tid] = 0;
   __syncthreads();
-  for (uint32_t base = i0; base < i1; base += 256) {
-    const uint32_t i = base + tid;
-    const bool on = i < i1;
-    uint32_t p = 0, h = 0;
-    if (on) sort_load<PASS>(A, b, i, p, h);
-    const uint32_t d = sort_digit<PASS>(h);
-    const unsigned act = __ballot_sync(kFull, on);
-    if (on) {
-      const unsigned peers = __match_any_sync(act, d);
-      if (lane == (uint32_t)__ffs(peers) - 1u) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+  const uint32_t i = i0 + 16 * tid;
+  if (i < i1) {
+    uint32_t h[16];
+    if (PASS == 0) {
+      const uint64_t a = A.in_off[b] + i;
+      const uint4* q16 = reinterpret_cast<const uint4*>(A.in + (a & ~(uint64_t)15));
+      const uint4 c0 = __ldg(q16), c1 = __ldg(q16 + 1), c2 = __ldg(q16 + 2);
+      const uint32_t w12[12] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w};
+      const uint32_t o = (uint32_t)(a >> 2) & 3u, sh = (uint32_t)(a & 3u) * 8u;
+      uint32_t u[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) u[k] = o == 0 ? w12[k] : o == 1 ? w12[k + 1] : o == 2 ? w12[k + 2] : w12[k + 3];
+      uint32_t x[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) x[k] = __funnelshift_r(u[k], u[k + 1], sh);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) h[j] = (__funnelshift_r(x[j >> 2], x[(j >> 2) + 1], 8 * (j & 3)) * 2654435761u) >> 16;
+    } else {
+      const uint4* q = reinterpret_cast<const uint4*>(A.tmp_h + (size_t)b * A.B + i);
+      const uint4 v0 = q[0], v1 = q[1];
+      const uint32_t vw[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+      for (int j = 0; j < 16; ++j) h[j] = (vw[j >> 1] >> (16 * (j & 1))) & 0xFFFFu;
     }
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (i + j < i1) atomicAdd(&hist[w][sort_digit<PASS>(h[j])], 1u);
   }
   __syncthreads();
-  A.scnt[((size_t)b * sort_tiles(A.B) + t) * 256 + tid] = hist[tid];
+  uint32_t sum = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) sum += hist[k][tid];
+  A.scnt[((size_t)b * sort_tiles(A.B) + t) * 256 + tid] = sum;
 }
 
 // per block: counts -> each tile's start per digit (digit-major order over the block's tiles)
@@ -519,24 +542,26 @@ __global__ void __launch_bounds__(256) k_enc_parse(EncArgs A) {
     }
     if (!__syncthreads_or(changed)) break;
   }
-  // tokens: count per segment, offsets, then write
+  // tokens: each segment's final walk writes them to its own slots (a token takes at least 4 bytes, so
+  // a segment of S bytes has at most S / 4 + 1), then they move to their offsets in the block's list
   const uint32_t from = ent[q];
+  const uint32_t slots = S / 4 + 2;
+  uint32_t* gi = A.tk_seg + (size_t)b * 3 * seg_tok_cap(A.B) + (size_t)q * slots;
+  uint32_t* gm = gi + seg_tok_cap(A.B);
+  uint32_t* gd = gm + seg_tok_cap(A.B);
   uint32_t cnt = 0;
   for (uint32_t p = from; __any_sync(kFull, p < e);) {
     p = warp_step(P, p, p < e, t, ta, tc, td);
-    cnt += t;
+    if (t) { gi[cnt] = ta; gm[cnt] = tc; gd[cnt] = td; ++cnt; }
   }
   const uint32_t incl = warp_incl_scan(cnt);
   if (lane_id() == 31) wsum[q >> 5] = incl;
   __syncthreads();
   uint32_t off = incl - cnt;
   for (uint32_t k = 0; k < (q >> 5); ++k) off += wsum[k];
-  const size_t to = (size_t)b * tok_cap(A.B);
-  for (uint32_t p = from; __any_sync(kFull, p < e);) {
-    p = warp_step(P, p, p < e, t, ta, tc, td);
-    if (t) { A.tk_i[to + off] = ta; A.tk_m[to + off] = tc; A.tk_d[to + off] = td; ++off; }
-  }
-  if (q == 255) A.bcnt[b * 8 + 0] = off;
+  const size_t to = (size_t)b * tok_cap(A.B) + off;
+  for (uint32_t k = 0; k < cnt; ++k) { A.tk_i[to + k] = gi[k]; A.tk_m[to + k] = gm[k]; A.tk_d[to + k] = gd[k]; }
+  if (q == 255) A.bcnt[b * 8 + 0] = off + cnt;
 }
 
 // ---------------------------------------------------------------- 4. tokens -> streams

@@ -78,6 +78,7 @@ struct EncArgs {
   uint32_t* scnt;                 // sort: per block ceil(B / 4096) * 256 tile digit counts / starts
   uint16_t *tmp_h, *srt_h;
   uint32_t *tk_i, *tk_m, *tk_d;   // tokens, tok_cap(B) per block
+  uint32_t* tk_seg;               // the parse's per-segment token slots: 3 * seg_tok_cap(B) per block
   uint32_t* bcnt;                 // per block [8]: nt, nl, ne, nob, ng, payload size, method
   uint8_t *s_lit, *s_tok, *s_ext, *s_sym, *s_grp, *s_bits;
   uint8_t* lanes;                 // rANS lane scratch, lanes_per_block(B) per block
@@ -110,6 +111,8 @@ __host__ __device__ inline uint64_t lane_base(uint32_t B, uint32_t s) {
 }
 __host__ __device__ inline uint64_t lanes_per_block(uint32_t B) { return lane_base(B, 5); }
 __host__ __device__ inline uint32_t bits_cap(uint32_t B) { return 5 * B / 8 + 64; }
+// the parse's token slots per block: 256 segments of ceil(B / 256) bytes, ceil(B / 256) / 4 + 2 each
+__host__ __device__ inline uint32_t seg_tok_cap(uint32_t B) { return 256 * (((B + 255) / 256) / 4 + 2); }
 
 void launch_encode(const EncArgs& A, const CrcArgs& crc_in, cudaStream_t st, Stages& S);
 constexpr uint32_t kMaxMatchTile = 1024;
