@@ -241,9 +241,10 @@ int ensure_dec(zc_ctx* c, uint32_t nb, uint32_t block_log) {
 
 bool bad_block_log(uint32_t bl) { return bl < zc::kMinBlockLog || bl > zc::kMaxBlockLog; }
 
-// blocks per encoder launch: about 256 MiB of input, and the grid's y limit
+// blocks per encoder launch: 1 GiB of input (about 28 GiB of scratch: several waves of every stage on
+// 148 SMs), and the grid's y limit
 uint32_t enc_blocks_per_launch(uint32_t block_log) {
-  return (uint32_t)std::min<size_t>(((size_t)256 << 20) >> block_log, 65535);
+  return (uint32_t)std::min<size_t>(((size_t)1 << 30) >> block_log, 65535);
 }
 uint32_t dec_blocks_per_launch(uint32_t block_log) {
   return (uint32_t)std::min<size_t>(((size_t)1 << 30) >> block_log, 1u << 20);
