@@ -746,7 +746,7 @@ def main():
     ap.add_argument("--pool", type=int, default=48, help="serve: distinct files the jobs draw from")
     ap.add_argument("--max-job-mib", type=int, default=256, help="serve: the largest job")
     ap.add_argument("--budget-gib", type=int, default=112, help="serve: device memory admission budget (GiB)")
-    ap.add_argument("--rates", default="4,8,16,32,64,128", help="serve: arrival rates to sweep (jobs/s)")
+    ap.add_argument("--rates", default="8,32,64,128,256,512", help="serve: arrival rates to sweep (jobs/s)")
     ap.add_argument("--duration", type=float, default=6.0, help="serve: seconds of arrivals per rate")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -1,5 +1,6 @@
 // zc_serve.cu -- the serving loop of include/zero_cuda.h: jobs admitted by free device memory, their
-// blocks batched across jobs tick by tick, each batch one replayed CUDA graph.  Host code only; the work
+// blocks batched across jobs tick by tick, each batch one replayed CUDA graph, two batches in flight (the
+// next one runs on the GPU while the host hands out the last one's results).  Host code only; the work
 // goes through the device entry points (zc_compress_device / zc_decompress_device) of one context.
 #include <cuda_runtime.h>
 
@@ -65,6 +66,7 @@ struct Job {
   std::vector<uint32_t> blen, rlen;                 // per block: input length, raw length
   uint64_t pay_at = 0;                              // compress: next free byte of the job's payload buffer
   uint64_t raw_total = 0;
+  cudaEvent_t up = nullptr;                         // recorded after the job's upload
 };
 
 // a batch's class: the kind of kernels, block size and level it shares
@@ -83,10 +85,28 @@ constexpr uint32_t kCap = 4096;  // blocks per batch at most (padded to a fixed 
 
 }  // namespace
 
+// one batch in flight: its descriptors and results (device, and pinned host), its payload / raw-byte
+// staging, and the event recorded after its small results are copied down
+struct Slot {
+  uint64_t *d_a64 = nullptr, *d_b64 = nullptr, *d_total = nullptr;
+  uint32_t *d_a32 = nullptr, *d_b32 = nullptr, *d_c32 = nullptr, *d_err = nullptr;
+  uint8_t *d_meth = nullptr, *d_stage = nullptr;
+  uint8_t* h = nullptr;        // pinned: descriptors up, results down
+  uint8_t* h_stage = nullptr;  // pinned: payloads (compress) or raw bytes (extract) down
+  cudaEvent_t ev = nullptr;
+  bool busy = false;
+  Cls k{};
+  std::vector<std::pair<Job*, uint32_t>> take;
+  std::vector<std::pair<uint64_t, uint64_t>> runs;  // extract: per run of a job's blocks, stage offset, length
+  int rc = ZC_OK;
+};
+
 struct zc_server {
   int device = 0;
   zc_ctx* ctx = nullptr;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr;   // kernels and small result copies, in order
+  cudaStream_t ust = nullptr;  // job uploads (the kernel stream waits on each job's upload event)
+  cudaStream_t cst = nullptr;  // payload copies of a finished batch, beside the next batch's kernels
   Arena arena;
   uint64_t max_batch = 256ull << 20;
   std::mutex mu;
@@ -98,12 +118,7 @@ struct zc_server {
   bool stop = false;
   std::thread worker;
   uint64_t jobs_done = 0, raw_bytes = 0, ticks = 0;
-  // batch descriptors and results, device and pinned host
-  uint64_t *d_a64 = nullptr, *d_b64 = nullptr, *d_total = nullptr;
-  uint32_t *d_a32 = nullptr, *d_b32 = nullptr, *d_c32 = nullptr, *d_err = nullptr;
-  uint8_t *d_meth = nullptr, *d_stage = nullptr;
-  uint8_t* h = nullptr;  // pinned: descriptors up, results down
-  uint8_t* h_stage = nullptr;
+  Slot slot[2];
   int failed = 0;  // a device failure ends the server: every job gets ZC_E_DEVICE
 };
 
@@ -113,15 +128,16 @@ uint32_t batch_cap(const zc_server* S, uint32_t bl) {
   return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(kCap, S->max_batch >> bl));
 }
 
-// places a job in the arena and starts its upload; false when it does not fit now
+// places a job in the arena and starts its upload on the upload stream; false when it does not fit now
 bool admit(zc_server* S, Job* J) {
   uint64_t off;
   if (!S->arena.alloc(J->footprint, off)) return false;
   J->in_off = off;
   J->out_off = off + Arena::round(J->j.in_len + 64);
   J->admitted = true;
-  if (J->j.in_len) cudaMemcpyAsync(S->arena.base + J->in_off, J->j.in, J->j.in_len, cudaMemcpyHostToDevice, S->st);
-  cudaMemsetAsync(S->arena.base + J->in_off + J->j.in_len, 0, 64, S->st);
+  if (J->j.in_len) cudaMemcpyAsync(S->arena.base + J->in_off, J->j.in, J->j.in_len, cudaMemcpyHostToDevice, S->ust);
+  cudaMemsetAsync(S->arena.base + J->in_off + J->j.in_len, 0, 64, S->ust);
+  if (cudaEventCreateWithFlags(&J->up, cudaEventDisableTiming) == cudaSuccess) cudaEventRecord(J->up, S->ust);
   return true;
 }
 
@@ -131,119 +147,184 @@ void finish(zc_server* S, Job* J, int status) {
   J->done = true;
   J->t_done = now_s();
   if (J->admitted) S->arena.release(J->in_off, J->footprint);
+  if (J->up) { cudaEventDestroy(J->up); J->up = nullptr; }
   S->jobs_done += 1;
   S->raw_bytes += J->raw_total;
 }
 
-// one tick: a batch of blocks of one class, from the admitted jobs in arrival order
-void run_batch(zc_server* S, const Cls& k, std::vector<std::pair<Job*, uint32_t>>& take) {
+// host views of a slot's pinned descriptor / result area
+struct Views {
+  uint64_t *ha, *hb;
+  uint32_t *h1, *h2;
+  uint8_t* hm;
+  uint64_t* r_off;
+  uint32_t *r_len, *r_crc, *r_err;
+  uint8_t* r_meth;
+  uint64_t* r_total;
+};
+Views views(Slot& L) {
+  Views v;
+  v.ha = reinterpret_cast<uint64_t*>(L.h);
+  v.hb = v.ha + kCap;
+  v.h1 = reinterpret_cast<uint32_t*>(v.hb + kCap);
+  v.h2 = v.h1 + kCap;
+  v.hm = reinterpret_cast<uint8_t*>(v.h2 + kCap);
+  v.r_off = reinterpret_cast<uint64_t*>(v.hm + kCap);
+  v.r_len = reinterpret_cast<uint32_t*>(v.r_off + kCap);
+  v.r_crc = v.r_len + kCap;
+  v.r_err = v.r_crc + kCap;
+  v.r_meth = reinterpret_cast<uint8_t*>(v.r_err + kCap);
+  v.r_total = reinterpret_cast<uint64_t*>(v.r_meth + kCap + 8);
+  return v;
+}
+
+// queues a tick's batch (blocks of one class, from the admitted jobs in arrival order) on the stream:
+// descriptors up, the batch's graph, small results down, the raw bytes of extract jobs to the stage;
+// returns without waiting
+void enqueue_batch(zc_server* S, Slot& L) {
+  const Cls& k = L.k;
   const uint32_t cap = batch_cap(S, k.bl);
-  uint64_t* ha = reinterpret_cast<uint64_t*>(S->h);          // cap: in / comp offsets
-  uint64_t* hb = ha + kCap;                                  // cap: out offsets (decode)
-  uint32_t* h1 = reinterpret_cast<uint32_t*>(hb + kCap);     // cap: lengths (in / comp)
-  uint32_t* h2 = h1 + kCap;                                  // cap: raw lengths (decode)
-  uint8_t* hm = reinterpret_cast<uint8_t*>(h2 + kCap);       // cap: methods
-  // results land after the descriptors
-  uint64_t* r_off = reinterpret_cast<uint64_t*>(hm + kCap);  // cap
-  uint32_t* r_len = reinterpret_cast<uint32_t*>(r_off + kCap);
-  uint32_t* r_crc = r_len + kCap;
-  uint32_t* r_err = r_crc + kCap;
-  uint8_t* r_meth = reinterpret_cast<uint8_t*>(r_err + kCap);
-  uint64_t* r_total = reinterpret_cast<uint64_t*>(r_meth + kCap + 8);
-  const uint32_t n = (uint32_t)take.size();
+  Views v = views(L);
+  const uint32_t n = (uint32_t)L.take.size();
   for (uint32_t i = 0; i < cap; ++i) {
     if (i < n) {
-      Job* J = take[i].first;
-      const uint32_t b = take[i].second;
-      ha[i] = J->in_off + J->bin[b];
-      hb[i] = J->out_off + J->bout[b];
-      h1[i] = J->blen[b];
-      h2[i] = J->rlen[b];
-      hm[i] = k.compress ? 0 : J->j.methods[b];
+      Job* J = L.take[i].first;
+      const uint32_t b = L.take[i].second;
+      v.ha[i] = J->in_off + J->bin[b];
+      v.hb[i] = J->out_off + J->bout[b];
+      v.h1[i] = J->blen[b];
+      v.h2[i] = J->rlen[b];
+      v.hm[i] = k.compress ? 0 : J->j.methods[b];
     } else {  // padding: an empty block
-      ha[i] = 0; hb[i] = 0; h1[i] = 0; h2[i] = 0; hm[i] = 0;
+      v.ha[i] = 0; v.hb[i] = 0; v.h1[i] = 0; v.h2[i] = 0; v.hm[i] = 0;
     }
   }
   cudaStream_t st = S->st;
-  cudaMemcpyAsync(S->d_a64, ha, cap * 8, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(S->d_b64, hb, cap * 8, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(S->d_a32, h1, cap * 4, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(S->d_b32, h2, cap * 4, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(S->d_meth, hm, cap, cudaMemcpyHostToDevice, st);
-  int rc;
+  L.rc = ZC_OK;
+  L.runs.clear();
+  for (uint32_t i = 0; i < n; ++i)
+    if (L.take[i].first->up && (i == 0 || L.take[i - 1].first != L.take[i].first))
+      cudaStreamWaitEvent(st, L.take[i].first->up, 0);
+  cudaMemcpyAsync(L.d_a64, v.ha, cap * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(L.d_b64, v.hb, cap * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(L.d_a32, v.h1, cap * 4, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(L.d_b32, v.h2, cap * 4, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(L.d_meth, v.hm, cap, cudaMemcpyHostToDevice, st);
   if (k.compress) {
-    rc = zc_compress_device(S->ctx, S->arena.base, S->d_a64, S->d_a32, cap, k.bl, k.level, S->d_meth, S->d_c32,
-                            S->d_err, S->d_stage, S->max_batch + 64, S->d_b64, S->d_total, st);
-    if (!rc) {
-      cudaMemcpyAsync(r_off, S->d_b64, cap * 8, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(r_len, S->d_c32, cap * 4, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(r_crc, S->d_err, cap * 4, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(r_meth, S->d_meth, cap, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(r_total, S->d_total, 8, cudaMemcpyDeviceToHost, st);
-      if (cudaStreamSynchronize(st) != cudaSuccess) rc = ZC_E_DEVICE;
+    L.rc = zc_compress_device(S->ctx, S->arena.base, L.d_a64, L.d_a32, cap, k.bl, k.level, L.d_meth, L.d_c32,
+                              L.d_err, L.d_stage, S->max_batch + 64, L.d_b64, L.d_total, st);
+    if (!L.rc) {
+      cudaMemcpyAsync(v.r_off, L.d_b64, cap * 8, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(v.r_len, L.d_c32, cap * 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(v.r_crc, L.d_err, cap * 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(v.r_meth, L.d_meth, cap, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(v.r_total, L.d_total, 8, cudaMemcpyDeviceToHost, st);
     }
-    if (!rc && *r_total) {
-      cudaMemcpyAsync(S->h_stage, S->d_stage, *r_total, cudaMemcpyDeviceToHost, st);
-      if (cudaStreamSynchronize(st) != cudaSuccess) rc = ZC_E_DEVICE;
+  } else {
+    L.rc = zc_decompress_device(S->ctx, S->arena.base, L.d_a64, L.d_a32, L.d_meth, L.d_b32, cap, k.bl,
+                                S->arena.base, L.d_b64, L.d_c32, L.d_err, st);
+    if (!L.rc) {
+      cudaMemcpyAsync(v.r_crc, L.d_c32, cap * 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(v.r_err, L.d_err, cap * 4, cudaMemcpyDeviceToHost, st);
+      // the raw bytes of extract jobs to the stage, one copy per run of a job's blocks
+      uint64_t at = 0;
+      for (uint32_t i = 0; i < n;) {
+        Job* J = L.take[i].first;
+        uint32_t e = i;
+        while (e < n && L.take[e].first == J) ++e;
+        uint64_t len = 0;
+        if (J->j.kind == ZC_JOB_EXTRACT) {
+          const uint32_t b0 = L.take[i].second, b1 = L.take[e - 1].second;
+          const uint64_t o0 = J->bout[b0], o1 = J->bout[b1] + J->rlen[b1];
+          len = o1 > o0 ? o1 - o0 : 0;
+          if (len) cudaMemcpyAsync(L.h_stage + at, S->arena.base + J->out_off + o0, len, cudaMemcpyDeviceToHost, st);
+        }
+        L.runs.emplace_back(at, len);
+        at += len;
+        i = e;
+      }
+    }
+  }
+  if (cudaEventRecord(L.ev, st) != cudaSuccess && !L.rc) L.rc = ZC_E_DEVICE;
+  L.busy = true;
+}
+
+// waits for a queued batch and hands its results to its jobs (payloads copied down on the second stream
+// while the next batch's kernels run)
+void complete_batch(zc_server* S, Slot& L) {
+  const Cls& k = L.k;
+  Views v = views(L);
+  const uint32_t n = (uint32_t)L.take.size();
+  int rc = L.rc;
+  if (!rc && cudaEventSynchronize(L.ev) != cudaSuccess) rc = ZC_E_DEVICE;
+  if (k.compress) {
+    if (!rc && *v.r_total) {
+      cudaMemcpyAsync(L.h_stage, L.d_stage, *v.r_total, cudaMemcpyDeviceToHost, S->cst);
+      if (cudaStreamSynchronize(S->cst) != cudaSuccess) rc = ZC_E_DEVICE;
     }
     for (uint32_t i = 0; i < n && !rc; ++i) {
-      Job* J = take[i].first;
-      const uint32_t b = take[i].second;
-      J->j.out_methods[b] = r_meth[i];
-      J->j.out_lens[b] = r_len[i];
-      if (J->j.out_crcs) J->j.out_crcs[b] = r_crc[i];
-      if (r_meth[i]) {
-        if (J->pay_at + r_len[i] > J->j.out_cap) { J->status = ZC_E_ARG; continue; }
-        memcpy(J->j.out + J->pay_at, S->h_stage + r_off[i], r_len[i]);
+      Job* J = L.take[i].first;
+      const uint32_t b = L.take[i].second;
+      J->j.out_methods[b] = v.r_meth[i];
+      J->j.out_lens[b] = v.r_len[i];
+      if (J->j.out_crcs) J->j.out_crcs[b] = v.r_crc[i];
+      if (v.r_meth[i]) {
+        if (J->pay_at + v.r_len[i] > J->j.out_cap) { J->status = ZC_E_ARG; continue; }
+        memcpy(J->j.out + J->pay_at, L.h_stage + v.r_off[i], v.r_len[i]);
         J->j.out_offs[b] = J->pay_at;
-        J->pay_at += r_len[i];
+        J->pay_at += v.r_len[i];
       } else {
         J->j.out_offs[b] = 0;
       }
     }
-  } else {
-    rc = zc_decompress_device(S->ctx, S->arena.base, S->d_a64, S->d_a32, S->d_meth, S->d_b32, cap, k.bl,
-                              S->arena.base, S->d_b64, S->d_c32, S->d_err, st);
-    if (!rc) {
-      cudaMemcpyAsync(r_crc, S->d_c32, cap * 4, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(r_err, S->d_err, cap * 4, cudaMemcpyDeviceToHost, st);
-      // the raw bytes of extract jobs, one copy per run of a job's blocks
-      for (uint32_t i = 0; i < n;) {
-        Job* J = take[i].first;
-        uint32_t e = i;
-        while (e < n && take[e].first == J) ++e;
-        if (J->j.kind == ZC_JOB_EXTRACT) {
-          const uint32_t b0 = take[i].second, b1 = take[e - 1].second;
-          const uint64_t o0 = J->bout[b0], o1 = J->bout[b1] + J->rlen[b1];
-          if (o1 > o0) cudaMemcpyAsync(J->j.out + o0, S->arena.base + J->out_off + o0, o1 - o0, cudaMemcpyDeviceToHost, st);
-        }
-        i = e;
-      }
-      if (cudaStreamSynchronize(st) != cudaSuccess) rc = ZC_E_DEVICE;
+  } else if (!rc) {
+    size_t run = 0;
+    for (uint32_t i = 0; i < n; ++run) {
+      Job* J = L.take[i].first;
+      uint32_t e = i;
+      while (e < n && L.take[e].first == J) ++e;
+      if (L.runs[run].second) memcpy(J->j.out + J->bout[L.take[i].second], L.h_stage + L.runs[run].first, L.runs[run].second);
+      i = e;
     }
-    for (uint32_t i = 0; i < n && !rc; ++i) {
-      Job* J = take[i].first;
-      const uint32_t b = take[i].second;
-      if (J->j.out_crcs) J->j.out_crcs[b] = r_crc[i];
-      if (r_err[i]) J->status = ZC_E_DATA;
-      else if (J->j.kind == ZC_JOB_TEST && J->j.crcs_expected && J->j.crcs_expected[b] != r_crc[i]) J->status = ZC_E_DATA;
+    for (uint32_t i = 0; i < n; ++i) {
+      Job* J = L.take[i].first;
+      const uint32_t b = L.take[i].second;
+      if (J->j.out_crcs) J->j.out_crcs[b] = v.r_crc[i];
+      if (v.r_err[i]) J->status = ZC_E_DATA;
+      else if (J->j.kind == ZC_JOB_TEST && J->j.crcs_expected && J->j.crcs_expected[b] != v.r_crc[i]) J->status = ZC_E_DATA;
     }
   }
   if (rc) S->failed = rc;
-  for (uint32_t i = 0; i < n; ++i) take[i].first->finished += 1;
+  for (uint32_t i = 0; i < n; ++i) L.take[i].first->finished += 1;
+  L.busy = false;
+  L.take.clear();
 }
 
+void finish_done(zc_server* S) {
+  for (auto it = S->active.begin(); it != S->active.end();) {
+    Job* J = *it;
+    if (J->finished == J->nb && J->next == J->nb) { finish(S, J, ZC_OK); it = S->active.erase(it); }
+    else ++it;
+  }
+  S->cv_done.notify_all();
+}
+
+// Each pass queues the next batch in one slot, then finishes the batch queued in the other slot on the
+// pass before: the GPU runs batch k + 1 while the host hands out batch k's results.
 void worker(zc_server* S) {
   cudaSetDevice(S->device);
   std::unique_lock<std::mutex> lk(S->mu);
+  int cur = 0;  // the slot the next batch goes to
   for (;;) {
+    const bool inflight = S->slot[0].busy || S->slot[1].busy;
     S->cv_work.wait(lk, [&] {
-      if (!S->pending.empty() || S->failed) return true;
+      if (inflight || !S->pending.empty() || S->failed) return true;
       for (Job* J : S->active) if (J->next < J->nb || J->finished == J->nb) return true;
       return S->stop && S->active.empty();
     });
-    if (S->stop && S->pending.empty() && S->active.empty()) return;
-    if (S->failed) {  // the GPU failed: everything left ends with the device error
+    if (S->stop && S->pending.empty() && S->active.empty() && !inflight) return;
+    if (S->failed) {  // the GPU failed: batches in flight end, then everything left ends with the error
+      for (Slot& L : S->slot) if (L.busy) { lk.unlock(); complete_batch(S, L); lk.lock(); }
       for (Job* J : S->active) finish(S, J, S->failed);
       for (Job* J : S->pending) finish(S, J, S->failed);
       S->active.clear();
@@ -258,41 +339,41 @@ void worker(zc_server* S) {
       S->active.push_back(S->pending.front());
       S->pending.pop_front();
     }
-    // the class of the oldest job with blocks left; then its blocks, and those of later jobs of the class
+    // the next batch: the class of the oldest job with blocks left; its blocks, then later jobs' of the class
+    bool queued = false;
+    Slot& L = S->slot[cur];
     Job* first = nullptr;
     for (Job* J : S->active) if (J->next < J->nb) { first = J; break; }
-    if (!first) {  // jobs with no blocks at all (empty input) finish at once
-      for (auto it = S->active.begin(); it != S->active.end();) {
-        if ((*it)->finished == (*it)->nb) { finish(S, *it, ZC_OK); it = S->active.erase(it); }
-        else ++it;
+    if (first && !L.busy) {
+      const Cls k = cls_of(first);
+      const uint32_t cap = batch_cap(S, k.bl);
+      L.k = k;
+      L.take.clear();
+      uint64_t bytes = 0;
+      for (Job* J : S->active) {
+        if (!(cls_of(J) == k)) continue;
+        while (J->next < J->nb && L.take.size() < cap) {
+          const uint64_t nbytes = (uint64_t)(k.compress ? J->blen[J->next] : J->rlen[J->next]);
+          if (!L.take.empty() && bytes + nbytes > S->max_batch) break;
+          L.take.emplace_back(J, J->next++);
+          bytes += nbytes;
+        }
+        if (L.take.size() >= cap || bytes >= S->max_batch) break;
       }
-      S->cv_done.notify_all();
-      continue;
+      lk.unlock();
+      enqueue_batch(S, L);
+      lk.lock();
+      S->ticks += 1;
+      queued = true;
     }
-    const Cls k = cls_of(first);
-    const uint32_t cap = batch_cap(S, k.bl);
-    std::vector<std::pair<Job*, uint32_t>> take;
-    uint64_t bytes = 0;
-    for (Job* J : S->active) {
-      if (!(cls_of(J) == k)) continue;
-      while (J->next < J->nb && take.size() < cap) {
-        const uint64_t nbytes = (uint64_t)(k.compress ? J->blen[J->next] : J->rlen[J->next]);
-        if (!take.empty() && bytes + nbytes > S->max_batch) break;
-        take.emplace_back(J, J->next++);
-        bytes += nbytes;
-      }
-      if (take.size() >= cap || bytes >= S->max_batch) break;
+    Slot& P = S->slot[cur ^ 1];
+    if (P.busy) {
+      lk.unlock();
+      complete_batch(S, P);
+      lk.lock();
     }
-    lk.unlock();
-    run_batch(S, k, take);
-    lk.lock();
-    S->ticks += 1;
-    for (auto it = S->active.begin(); it != S->active.end();) {
-      Job* J = *it;
-      if (J->finished == J->nb) { finish(S, J, ZC_OK); it = S->active.erase(it); }
-      else ++it;
-    }
-    S->cv_done.notify_all();
+    if (queued) cur ^= 1;
+    finish_done(S);
   }
 }
 
@@ -310,21 +391,26 @@ int zc_serve_open(zc_server** out, int device, uint64_t budget_bytes, uint64_t m
   if (rc) { zc_close(S->ctx); delete S; return rc; }
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->ust, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->cst, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&S->arena.base, std::max<uint64_t>(budget_bytes, 1u << 20));
   if (e == cudaSuccess) {
     S->arena.size = std::max<uint64_t>(budget_bytes, 1u << 20);
     S->arena.free_[0] = S->arena.size;
   }
-  if (e == cudaSuccess) e = cudaMalloc(&S->d_a64, kCap * 8 * 3);
-  if (e == cudaSuccess) { S->d_b64 = S->d_a64 + kCap; S->d_total = S->d_b64 + kCap; }
-  if (e == cudaSuccess) e = cudaMalloc(&S->d_a32, kCap * 4 * 4 + kCap);
-  if (e == cudaSuccess) {
-    S->d_b32 = S->d_a32 + kCap; S->d_c32 = S->d_b32 + kCap; S->d_err = S->d_c32 + kCap;
-    S->d_meth = reinterpret_cast<uint8_t*>(S->d_err + kCap);
+  for (Slot& L : S->slot) {
+    if (e == cudaSuccess) e = cudaMalloc(&L.d_a64, kCap * 8 * 3);
+    if (e == cudaSuccess) { L.d_b64 = L.d_a64 + kCap; L.d_total = L.d_b64 + kCap; }
+    if (e == cudaSuccess) e = cudaMalloc(&L.d_a32, kCap * 4 * 4 + kCap);
+    if (e == cudaSuccess) {
+      L.d_b32 = L.d_a32 + kCap; L.d_c32 = L.d_b32 + kCap; L.d_err = L.d_c32 + kCap;
+      L.d_meth = reinterpret_cast<uint8_t*>(L.d_err + kCap);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&L.d_stage, S->max_batch + 64);
+    if (e == cudaSuccess) e = cudaMallocHost(&L.h, kCap * 64 + 64);
+    if (e == cudaSuccess) e = cudaMallocHost(&L.h_stage, S->max_batch + 64);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming);
   }
-  if (e == cudaSuccess) e = cudaMalloc(&S->d_stage, S->max_batch + 64);
-  if (e == cudaSuccess) e = cudaMallocHost(&S->h, kCap * 64 + 64);
-  if (e == cudaSuccess) e = cudaMallocHost(&S->h_stage, S->max_batch + 64);
   if (e == cudaSuccess) rc = zc_set_graphs(S->ctx, 1);
   if (e != cudaSuccess || rc) {
     zc_serve_close(S);
@@ -346,15 +432,23 @@ void zc_serve_close(zc_server* S) {
     S->worker.join();
   }
   cudaSetDevice(S->device);
-  if (S->st) cudaStreamSynchronize(S->st);
-  for (auto& kv : S->jobs) delete kv.second;
+  for (cudaStream_t x : {S->st, S->ust, S->cst})
+    if (x) cudaStreamSynchronize(x);
+  for (auto& kv : S->jobs) {
+    if (kv.second->up) cudaEventDestroy(kv.second->up);
+    delete kv.second;
+  }
   if (S->arena.base) cudaFree(S->arena.base);
-  if (S->d_a64) cudaFree(S->d_a64);
-  if (S->d_a32) cudaFree(S->d_a32);
-  if (S->d_stage) cudaFree(S->d_stage);
-  if (S->h) cudaFreeHost(S->h);
-  if (S->h_stage) cudaFreeHost(S->h_stage);
-  if (S->st) cudaStreamDestroy(S->st);
+  for (Slot& L : S->slot) {
+    if (L.d_a64) cudaFree(L.d_a64);
+    if (L.d_a32) cudaFree(L.d_a32);
+    if (L.d_stage) cudaFree(L.d_stage);
+    if (L.h) cudaFreeHost(L.h);
+    if (L.h_stage) cudaFreeHost(L.h_stage);
+    if (L.ev) cudaEventDestroy(L.ev);
+  }
+  for (cudaStream_t x : {S->st, S->ust, S->cst})
+    if (x) cudaStreamDestroy(x);
   zc_close(S->ctx);
   delete S;
 }
