@@ -31,6 +31,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "zero-compression_b200"))
 
 METRIC = "compress/decompress GB/s on 1 B200, bit-exact round-trip; served p50/p99 latency"
+# dram__bytes_read.sum + dram__bytes_write.sum per raw byte of one launch (block 18, level 5 lz_mix), from
+# the ncu captures summarised in profiles/encoder_kernels_lz256m_b18_l5.md (256 MiB launch) and
+# profiles/decoder_kernels_lz512m_b18_l5.md (512 MiB launch)
+DRAM_BYTES_PER_RAW_BYTE = {"k_enc_match": 10.885, "k_enc_parse": 20.72, "k_sort_scatter": 9.557,
+                           "k_dec_fill": 1.760, "k_dec_tokens": 0.285, "k_dec_streams": 0.283}
 GB = 1e9
 
 
@@ -294,14 +299,10 @@ def run_ours(args):
     dom_name, (dom_ms, dom_launches) = dom
     steps_bytes = (n + comp_bytes) * args.steps
     achieved = steps_bytes / (dom_ms * 1e-3) / GB if dom_ms else 0.0
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
-            tr = json.load(f)
-        if dom_name in tr:
-            traffic = int(tr[dom_name]["dram_bytes_per_input_byte"] * n / max(1, dom_launches // args.steps))
-    except Exception:
-        traffic = None
+    # DRAM traffic of one launch: ncu's dram bytes per raw byte for the kernel (a capture of the same
+    # kernel on a smaller launch; traffic grows with the blocks processed), times the raw bytes per launch
+    per_byte = DRAM_BYTES_PER_RAW_BYTE.get(dom_name)
+    traffic = int(per_byte * n / max(1, dom_launches // args.steps)) if per_byte else None
     total_stage_ms = sum(v[0] for v in stages.values()) or 1.0
     pipe_achieved = steps_bytes / (tot_ms * 1e-3) / GB
 
@@ -627,6 +628,8 @@ def run_decode(args):
             "ratio": round(comp / n, 5), "bit_exact": ok, "compress_s_untimed": round(t_comp, 3),
             "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": int(per_launch),
+                         "traffic": (int(DRAM_BYTES_PER_RAW_BYTE[dom[0]] * n / max(1, dom[1][1] // max(1, args.steps)))
+                                     if dom[0] in DRAM_BYTES_PER_RAW_BYTE else None),
                          "pipeline_frac": round((n + comp) / (t * 1e-3) / GB / peak, 4)},
             "stages_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in stages.items()},
             "gpu_launches": int(launches), "clocks": clk.summary()}
