@@ -738,9 +738,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--block", type=int, default=18)
-    ap.add_argument("--level", type=int, default=5)
-    ap.add_argument("--size-mib", type=int, default=1024)
+    ap.add_argument("--block", type=int, default=None, help="default 18; 20 for --config decode")
+    ap.add_argument("--level", type=int, default=None, help="default 5; 9 for --config decode")
+    ap.add_argument("--size-mib", type=int, default=None, help="default 1024; 8192 for --config decode")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--config", choices=["lz", "batched", "decode", "serve"], default="lz",
                     help="lz: the headline round trip; batched: many files, plain vs batched; decode: extract-heavy")
@@ -752,6 +752,13 @@ def main():
     ap.add_argument("--rates", default="8,32,64,128,256,512", help="serve: arrival rates to sweep (jobs/s)")
     ap.add_argument("--duration", type=float, default=6.0, help="serve: seconds of arrivals per rate")
     args = ap.parse_args()
+    dec = args.config == "decode"  # the decode-heavy workload: an 8 GiB archive at block 20, level 9
+    if args.block is None:
+        args.block = 20 if dec else 18
+    if args.level is None:
+        args.level = 9 if dec else 5
+    if args.size_mib is None:
+        args.size_mib = 8192 if dec else 1024
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "batched":

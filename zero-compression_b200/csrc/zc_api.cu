@@ -246,8 +246,10 @@ bool bad_block_log(uint32_t bl) { return bl < zc::kMinBlockLog || bl > zc::kMaxB
 uint32_t enc_blocks_per_launch(uint32_t block_log) {
   return (uint32_t)std::min<size_t>(((size_t)1 << 30) >> block_log, 65535);
 }
+// blocks per decoder launch: 4 GiB of output (the fill runs one warp per block, so large launches keep
+// every SM busy; about 6 bytes of scratch per output byte)
 uint32_t dec_blocks_per_launch(uint32_t block_log) {
-  return (uint32_t)std::min<size_t>(((size_t)1 << 30) >> block_log, 1u << 20);
+  return (uint32_t)std::min<size_t>(((size_t)4 << 30) >> block_log, 1u << 20);
 }
 
 int check_launch(zc_ctx* c, const char* what) {
