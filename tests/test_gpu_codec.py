@@ -268,3 +268,39 @@ def test_launch_shapes_never_change_bytes(codec):
         for bl, s in default.items():
             codec.set_shape(bl, 5, **s)
         codec.prepare(18)
+
+
+def test_host_calls_in_chunks_match_one_device_call(codec):
+    """Host-buffer calls over more than one chunk (their copies overlap the other chunk's kernels) give
+    the bytes one device-resident call gives, and round-trip."""
+    import torch
+    import datagen as G
+    dev = torch.device("cuda", 0)
+    bl, B = 18, 1 << 18
+    data = np.concatenate([G.lz_mix(256 << 20, bl, 81), G.lz_mix(256 << 20, bl, 82), G.text_mix((8 << 20) + 12345, 83)])
+    n, nb = data.size, (data.size + B - 1) // B
+    meth, lens, crcs, pay, offs = codec.compress_arrays(data, bl, level=5)
+    d_in = torch.zeros(n + 64, dtype=torch.uint8, device=dev)
+    d_in[:n] = torch.from_numpy(data).to(dev)
+    doffs = torch.arange(nb, dtype=torch.int64, device=dev) * B
+    dlens = torch.clamp(n - doffs, max=B).to(torch.int32)
+    m = torch.zeros(nb, dtype=torch.uint8, device=dev)
+    l = torch.zeros(nb, dtype=torch.int32, device=dev)
+    c = torch.zeros(nb, dtype=torch.int32, device=dev)
+    o = torch.zeros(n + 64, dtype=torch.uint8, device=dev)
+    f = torch.zeros(nb, dtype=torch.int64, device=dev)
+    t = torch.zeros(1, dtype=torch.int64, device=dev)
+    codec.compress_device(d_in, doffs, dlens, nb, bl, m, l, c, o, f, t)
+    torch.cuda.synchronize()
+    assert np.array_equal(meth, m.cpu().numpy()) and np.array_equal(lens, l.cpu().numpy().astype(np.uint32))
+    assert np.array_equal(crcs, c.cpu().numpy().astype(np.uint32))
+    ho, hf = o.cpu().numpy(), f.cpu().numpy()
+    for b in range(nb):
+        if meth[b]:
+            assert pay[int(offs[b]): int(offs[b]) + int(lens[b])].tobytes() == ho[hf[b]: hf[b] + int(lens[b])].tobytes()
+    comp = [pay[int(offs[b]): int(offs[b]) + int(lens[b])] if meth[b] else data[b * B:(b + 1) * B] for b in range(nb)]
+    blob = np.concatenate(comp)
+    coffs = np.cumsum([0] + [x.size for x in comp[:-1]])
+    raw, dcrcs, errs = codec.decompress_arrays(blob, coffs, [x.size for x in comp], meth,
+                                               [min(B, n - b * B) for b in range(nb)])
+    assert not errs.any() and np.array_equal(raw[:n], data) and np.array_equal(dcrcs, crcs)

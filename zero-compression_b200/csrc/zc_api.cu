@@ -139,6 +139,14 @@ struct zc_ctx {
   // staging for the host-pointer calls
   DevBuf s_in, s_blk, s_out, s_meta;
   HostBuf h_meta;
+  // the host-pointer codec calls run in chunks through two stages: a chunk's copies (on cstream) overlap
+  // the other chunk's kernels (on stream)
+  struct Stage {
+    DevBuf in, blk, out, meta;
+    HostBuf h;  // descriptors up, then results down
+    cudaEvent_t ev_in = nullptr, ev_done = nullptr;
+  } pipe[2];
+  cudaStream_t cstream = nullptr;
 };
 
 namespace {
@@ -352,16 +360,56 @@ int with_graph(zc_ctx* c, int kind, const uint64_t* key, int nkey, cudaStream_t 
 }
 
 // host-pointer compress of nb blocks whose bytes lie in host memory [lo, lo + span)
+// blocks in chunk `i` of a host-pointer call: 128 MiB first (so the first kernels start early and the
+// copies left exposed are short), then 512 MiB, so that a large call's copies overlap kernels
+uint32_t host_chunk_blocks(uint32_t block_log, uint32_t per_launch, uint32_t i) {
+  const size_t bytes = (size_t)(i == 0 ? 128 : 512) << 20;
+  return std::max<uint32_t>(1, std::min<uint32_t>(per_launch, (uint32_t)(bytes >> block_log)));
+}
+
+// Compression of host-resident blocks in chunks through the two stages: chunk i's upload (copy stream)
+// overlaps chunk i-1's kernels, and chunk i-1's results come down while chunk i's kernels run.
 int compress_host(zc_ctx* c, const uint8_t* host_base, const uint64_t* in_offs, const uint32_t* in_lens, uint32_t nb,
                   uint64_t plain_n, uint32_t block_log, int level, uint8_t* methods, uint32_t* comp_lens,
                   uint32_t* crcs, uint8_t* payloads, size_t payload_cap, uint64_t* pay_offs) {
   if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
   const uint32_t B = 1u << block_log;
-  const uint32_t per = enc_blocks_per_launch(block_log);
-  cudaStream_t st = c->stream;
+  const uint32_t per_launch = enc_blocks_per_launch(block_log);
+  cudaStream_t st = c->stream, cs = c->cstream;
   uint64_t pay_at = 0;
-  for (uint32_t b0 = 0; b0 < nb; b0 += per) {
-    const uint32_t k = std::min(per, nb - b0);
+  struct Chunk { uint32_t b0 = 0, k = 0; size_t meta_at = 0, meta_bytes = 0; };
+  Chunk prev;
+  bool have_prev = false;
+  // the results of a finished chunk: counts first, then the payloads they size
+  auto harvest = [&](zc_ctx::Stage& S, const Chunk& q) -> int {
+    ZC_CUDA(cudaStreamWaitEvent(cs, S.ev_done, 0));
+    uint8_t* hm = static_cast<uint8_t*>(S.h.p) + q.meta_at;
+    ZC_CUDA(cudaMemcpyAsync(hm, S.meta.p, q.meta_bytes, cudaMemcpyDeviceToHost, cs));
+    ZC_CUDA(cudaStreamSynchronize(cs));
+    const uint64_t* h_poff = reinterpret_cast<const uint64_t*>(hm);
+    const uint64_t total = h_poff[q.k];
+    const uint32_t* h_plen = reinterpret_cast<const uint32_t*>(h_poff + q.k + 1);
+    const uint32_t* h_crc = h_plen + q.k;
+    const uint8_t* h_meth = reinterpret_cast<const uint8_t*>(h_crc + q.k);
+    if (pay_at + total > payload_cap) return fail(c, ZC_E_ARG, "payload buffer too small");
+    if (total) ZC_CUDA(cudaMemcpyAsync(payloads + pay_at, S.out.p, total, cudaMemcpyDeviceToHost, cs));
+    for (uint32_t b = 0; b < q.k; ++b) {
+      methods[q.b0 + b] = h_meth[b];
+      comp_lens[q.b0 + b] = h_plen[b];
+      if (crcs) crcs[q.b0 + b] = h_crc[b];
+      if (pay_offs) pay_offs[q.b0 + b] = h_meth[b] ? pay_at + h_poff[b] : 0;
+    }
+    ZC_CUDA(cudaStreamSynchronize(cs));
+    pay_at += total;
+    return ZC_OK;
+  };
+  uint32_t it = 0;
+  for (uint32_t b0 = 0; b0 < nb; b0 += prev.k, ++it) {
+    zc_ctx::Stage& S = c->pipe[it & 1];
+    Chunk q;
+    q.b0 = b0;
+    q.k = std::min(host_chunk_blocks(block_log, per_launch, it), nb - b0);
+    const uint32_t k = q.k;
     // the bytes of blocks b0 .. b0+k-1 as one host span
     uint64_t lo, hi;
     if (in_offs) {
@@ -377,55 +425,50 @@ int compress_host(zc_ctx* c, const uint8_t* host_base, const uint64_t* in_offs, 
       hi = std::min<uint64_t>(plain_n, (uint64_t)(b0 + k) * B);
     }
     const uint64_t span = hi - lo;
-    ZC_CUDA(grow(c->s_in, span + 64));
-    ZC_CUDA(grow(c->s_blk, (size_t)k * 12));
-    ZC_CUDA(grow(c->s_out, span + 64));
-    const size_t meta_bytes = (size_t)k * (8 + 4 + 4 + 1) + 16;
-    ZC_CUDA(grow(c->s_meta, meta_bytes));
-    ZC_CUDA(grow_host(c->h_meta, meta_bytes + (size_t)k * 12));
-    uint8_t* d_in = c->s_in.as<uint8_t>();
-    uint64_t* d_off = c->s_blk.as<uint64_t>();
+    q.meta_bytes = (size_t)k * (8 + 4 + 4 + 1) + 16;
+    q.meta_at = ((size_t)k * 12 + 255) & ~(size_t)255;
+    ZC_CUDA(grow(S.in, span + 64));
+    ZC_CUDA(grow(S.blk, (size_t)k * 12));
+    ZC_CUDA(grow(S.out, span + 64));
+    ZC_CUDA(grow(S.meta, q.meta_bytes));
+    ZC_CUDA(grow_host(S.h, q.meta_at + q.meta_bytes));
+    uint8_t* d_in = S.in.as<uint8_t>();
+    uint64_t* d_off = S.blk.as<uint64_t>();
     uint32_t* d_len = reinterpret_cast<uint32_t*>(d_off + k);
-    ZC_CUDA(cudaMemcpyAsync(d_in, host_base + lo, span, cudaMemcpyHostToDevice, st));
-    ZC_CUDA(cudaMemsetAsync(d_in + span, 0, 64, st));
+    // upload on the copy stream (the stage's last chunk was harvested, so its buffers are free)
+    ZC_CUDA(cudaMemcpyAsync(d_in, host_base + lo, span, cudaMemcpyHostToDevice, cs));
+    ZC_CUDA(cudaMemsetAsync(d_in + span, 0, 64, cs));
     if (in_offs) {
-      uint64_t* ho = static_cast<uint64_t*>(c->h_meta.p);
+      uint64_t* ho = static_cast<uint64_t*>(S.h.p);
       uint32_t* hl = reinterpret_cast<uint32_t*>(ho + k);
       for (uint32_t b = 0; b < k; ++b) { ho[b] = in_offs[b0 + b] - lo; hl[b] = in_lens[b0 + b]; }
-      ZC_CUDA(cudaMemcpyAsync(d_off, ho, (size_t)k * 12, cudaMemcpyHostToDevice, st));
-    } else {
+      ZC_CUDA(cudaMemcpyAsync(d_off, ho, (size_t)k * 12, cudaMemcpyHostToDevice, cs));
+    }
+    ZC_CUDA(cudaEventRecord(S.ev_in, cs));
+    // kernels on the compute stream once the upload is in
+    ZC_CUDA(cudaStreamWaitEvent(st, S.ev_in, 0));
+    if (!in_offs) {
       c->stages.begin("k_plain_blocks", st);
       k_plain_blocks<<<(k + 255) / 256, 256, 0, st>>>(span, B, k, d_off, d_len);
       c->stages.end(st);
     }
-    uint8_t* m = c->s_meta.as<uint8_t>();
+    uint8_t* m = S.meta.as<uint8_t>();
     uint64_t* d_poff = reinterpret_cast<uint64_t*>(m);
     uint64_t* d_total = d_poff + k;
     uint32_t* d_plen = reinterpret_cast<uint32_t*>(d_total + 1);
     uint32_t* d_crc = d_plen + k;
     uint8_t* d_meth = reinterpret_cast<uint8_t*>(d_crc + k);
-    if (int r = encode_device(c, d_in, d_off, d_len, k, block_log, level, d_meth, d_plen, d_crc, c->s_out.as<uint8_t>(),
-                              c->s_out.n, d_poff, d_total, 0, st))
+    if (int r = encode_device(c, d_in, d_off, d_len, k, block_log, level, d_meth, d_plen, d_crc, S.out.as<uint8_t>(),
+                              S.out.n, d_poff, d_total, 0, st))
       return r;
-    ZC_CUDA(cudaMemcpyAsync(c->h_meta.p, m, meta_bytes, cudaMemcpyDeviceToHost, st));
-    ZC_CUDA(cudaStreamSynchronize(st));
-    const uint8_t* hm = static_cast<const uint8_t*>(c->h_meta.p);
-    const uint64_t* h_poff = reinterpret_cast<const uint64_t*>(hm);
-    const uint64_t total = h_poff[k];
-    const uint32_t* h_plen = reinterpret_cast<const uint32_t*>(h_poff + k + 1);
-    const uint32_t* h_crc = h_plen + k;
-    const uint8_t* h_meth = reinterpret_cast<const uint8_t*>(h_crc + k);
-    if (pay_at + total > payload_cap) return fail(c, ZC_E_ARG, "payload buffer too small");
-    if (total) ZC_CUDA(cudaMemcpyAsync(payloads + pay_at, c->s_out.p, total, cudaMemcpyDeviceToHost, st));
-    for (uint32_t b = 0; b < k; ++b) {
-      methods[b0 + b] = h_meth[b];
-      comp_lens[b0 + b] = h_plen[b];
-      if (crcs) crcs[b0 + b] = h_crc[b];
-      if (pay_offs) pay_offs[b0 + b] = h_meth[b] ? pay_at + h_poff[b] : 0;
-    }
-    ZC_CUDA(cudaStreamSynchronize(st));
-    pay_at += total;
+    ZC_CUDA(cudaEventRecord(S.ev_done, st));
+    if (have_prev)
+      if (int r = harvest(c->pipe[(it - 1) & 1], prev)) return r;
+    prev = q;
+    have_prev = true;
   }
+  if (have_prev)
+    if (int r = harvest(c->pipe[(it - 1) & 1], prev)) return r;
   return ZC_OK;
 }
 
@@ -448,6 +491,11 @@ int zc_open(zc_ctx** out, int device) {
     return ZC_E_DEVICE;
   }
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking);
+  for (auto& S : c->pipe) {
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S.ev_in, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S.ev_done, cudaEventDisableTiming);
+  }
   if (e == cudaSuccess) e = zc::prepare_kernels();
   if (e == cudaSuccess) e = cudaMalloc(&c->d_crct, sizeof(zc::CrcTables));
   if (e == cudaSuccess) {
@@ -467,6 +515,7 @@ void zc_close(zc_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->cstream) cudaStreamSynchronize(c->cstream);
   drop_graphs(c);
   for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_minfo, &c->e_scnt, &c->e_tk_seg, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
                     &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
@@ -474,8 +523,15 @@ void zc_close(zc_ctx* c) {
                     &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta})
     release(*b);
   if (c->h_meta.p) cudaFreeHost(c->h_meta.p);
+  for (auto& S : c->pipe) {
+    for (DevBuf* b : {&S.in, &S.blk, &S.out, &S.meta}) release(*b);
+    if (S.h.p) cudaFreeHost(S.h.p);
+    if (S.ev_in) cudaEventDestroy(S.ev_in);
+    if (S.ev_done) cudaEventDestroy(S.ev_done);
+  }
   if (c->d_crct) cudaFree(c->d_crct);
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->cstream) cudaStreamDestroy(c->cstream);
   delete c;
 }
 
@@ -733,6 +789,8 @@ int zc_autotune(zc_ctx* c, const uint8_t* sample, size_t n, uint32_t block_log, 
   return r;
 }
 
+// Decompression of host-resident records in chunks through the two stages: chunk i's upload and
+// kernels overlap the download of chunk i-1's raw bytes.
 int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, const uint32_t* comp_lens,
                   const uint8_t* methods, const uint32_t* raw_lens, uint32_t nb, uint8_t* out, uint32_t* crcs_out,
                   uint32_t* block_err) {
@@ -743,12 +801,44 @@ int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, con
   uint32_t bl = zc::kMinBlockLog;
   while (bl < zc::kMaxBlockLog && (1u << bl) < maxraw) ++bl;
   if (maxraw > (1u << zc::kMaxBlockLog)) return fail(c, ZC_E_DATA, "a block is longer than 1 MiB");
-  const uint32_t per = dec_blocks_per_launch(bl);
-  cudaStream_t st = c->stream;
-  uint64_t out_at = 0;
+  const uint32_t per_launch = dec_blocks_per_launch(bl);
+  cudaStream_t st = c->stream, cs = c->cstream;
+  const size_t per_blk = 8 + 8 + 4 + 4 + 4 + 4 + 1;
   int status = ZC_OK;
-  for (uint32_t b0 = 0; b0 < nb; b0 += per) {
-    const uint32_t k = std::min(per, nb - b0);
+  struct Chunk { uint32_t b0 = 0, k = 0; uint64_t out_at = 0, raw_total = 0; };
+  Chunk prev;
+  bool have_prev = false;
+  // a finished chunk: its raw bytes and per-block CRCs / statuses come down on the copy stream
+  auto harvest = [&](zc_ctx::Stage& S, const Chunk& q) -> int {
+    uint8_t* hb = static_cast<uint8_t*>(S.h.p);
+    uint32_t* h_crc = reinterpret_cast<uint32_t*>(hb + (size_t)q.k * 16 + (size_t)q.k * 8);
+    uint32_t* h_err = h_crc + q.k;
+    uint8_t* db = S.blk.as<uint8_t>();
+    ZC_CUDA(cudaStreamWaitEvent(cs, S.ev_done, 0));
+    if (q.raw_total) ZC_CUDA(cudaMemcpyAsync(out + q.out_at, S.out.p, q.raw_total, cudaMemcpyDeviceToHost, cs));
+    ZC_CUDA(cudaMemcpyAsync(h_crc, db + (size_t)q.k * 24, (size_t)q.k * 8, cudaMemcpyDeviceToHost, cs));
+    ZC_CUDA(cudaStreamSynchronize(cs));
+    for (uint32_t b = 0; b < q.k; ++b) {
+      if (crcs_out) crcs_out[q.b0 + b] = h_crc[b];
+      if (block_err) block_err[q.b0 + b] = h_err[b];
+      if (h_err[b] && status == ZC_OK) {
+        status = ZC_E_DATA;
+        char m[128];
+        snprintf(m, sizeof m, "block %u damaged (GPU decoder, code %u)", q.b0 + b, h_err[b]);
+        c->err = m;
+      }
+    }
+    return ZC_OK;
+  };
+  uint64_t out_at = 0;
+  uint32_t it = 0;
+  for (uint32_t b0 = 0; b0 < nb; b0 += prev.k, ++it) {
+    zc_ctx::Stage& S = c->pipe[it & 1];
+    Chunk q;
+    q.b0 = b0;
+    q.k = std::min(host_chunk_blocks(bl, per_launch, it), nb - b0);
+    q.out_at = out_at;
+    const uint32_t k = q.k;
     uint64_t lo = UINT64_MAX, hi = 0, raw_total = 0, comp_sum = 0;
     for (uint32_t b = b0; b < b0 + k; ++b) {
       lo = std::min(lo, comp_offs[b]);
@@ -757,22 +847,21 @@ int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, con
       comp_sum += comp_lens[b];
     }
     if (lo == UINT64_MAX) lo = hi = 0;
+    q.raw_total = raw_total;
     // one copy of the span when the blocks lie close together (an archive's records), else gathered
     const bool gather = hi - lo > comp_sum + comp_sum / 2 + 4096;
     const uint64_t span = gather ? comp_sum : hi - lo;
-    ZC_CUDA(grow(c->s_in, span + 64));
-    ZC_CUDA(grow(c->s_out, raw_total + 64));
-    const size_t per_blk = 8 + 8 + 4 + 4 + 4 + 4 + 1;
-    ZC_CUDA(grow(c->s_blk, (size_t)k * per_blk + 64));
-    ZC_CUDA(grow_host(c->h_meta, (size_t)k * per_blk + 64 + (gather ? 0 : 0)));
-    uint8_t* hb = static_cast<uint8_t*>(c->h_meta.p);
+    ZC_CUDA(grow(S.in, span + 64));
+    ZC_CUDA(grow(S.out, raw_total + 64));
+    ZC_CUDA(grow(S.blk, (size_t)k * per_blk + 64));
+    ZC_CUDA(grow_host(S.h, (size_t)k * per_blk + 64));
+    // descriptors: comp offsets, out offsets (u64); comp lens, raw lens, crcs, errs (u32); methods (u8)
+    uint8_t* hb = static_cast<uint8_t*>(S.h.p);
     uint64_t* h_coff = reinterpret_cast<uint64_t*>(hb);
     uint64_t* h_ooff = h_coff + k;
     uint32_t* h_clen = reinterpret_cast<uint32_t*>(h_ooff + k);
     uint32_t* h_rlen = h_clen + k;
-    uint32_t* h_crc = h_rlen + k;
-    uint32_t* h_err = h_crc + k;
-    uint8_t* h_meth = reinterpret_cast<uint8_t*>(h_err + k);
+    uint8_t* h_meth = reinterpret_cast<uint8_t*>(h_rlen + 3 * (size_t)k);
     uint64_t g = 0, o = 0;
     for (uint32_t b = 0; b < k; ++b) {
       const uint32_t j = b0 + b;
@@ -784,16 +873,17 @@ int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, con
       h_rlen[b] = raw_lens[j];
       h_meth[b] = methods[j];
     }
-    uint8_t* d_in = c->s_in.as<uint8_t>();
+    uint8_t* d_in = S.in.as<uint8_t>();
     if (gather) {
       for (uint32_t b = 0; b < k; ++b)
         if (comp_lens[b0 + b])
-          ZC_CUDA(cudaMemcpyAsync(d_in + h_coff[b], comp + comp_offs[b0 + b], comp_lens[b0 + b], cudaMemcpyHostToDevice, st));
+          ZC_CUDA(cudaMemcpyAsync(d_in + h_coff[b], comp + comp_offs[b0 + b], comp_lens[b0 + b], cudaMemcpyHostToDevice, cs));
     } else if (span) {
-      ZC_CUDA(cudaMemcpyAsync(d_in, comp + lo, span, cudaMemcpyHostToDevice, st));
+      ZC_CUDA(cudaMemcpyAsync(d_in, comp + lo, span, cudaMemcpyHostToDevice, cs));
     }
-    uint8_t* db = c->s_blk.as<uint8_t>();
-    ZC_CUDA(cudaMemcpyAsync(db, hb, (size_t)k * per_blk, cudaMemcpyHostToDevice, st));
+    uint8_t* db = S.blk.as<uint8_t>();
+    ZC_CUDA(cudaMemcpyAsync(db, hb, (size_t)k * per_blk, cudaMemcpyHostToDevice, cs));
+    ZC_CUDA(cudaEventRecord(S.ev_in, cs));
     uint64_t* d_coff = reinterpret_cast<uint64_t*>(db);
     uint64_t* d_ooff = d_coff + k;
     uint32_t* d_clen = reinterpret_cast<uint32_t*>(d_ooff + k);
@@ -801,24 +891,19 @@ int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, con
     uint32_t* d_crc = d_rlen + k;
     uint32_t* d_err = d_crc + k;
     uint8_t* d_meth = reinterpret_cast<uint8_t*>(d_err + k);
-    if (int r = decode_device(c, d_in, d_coff, d_clen, d_meth, d_rlen, k, bl, c->s_out.as<uint8_t>(), d_ooff, d_crc,
+    ZC_CUDA(cudaStreamWaitEvent(st, S.ev_in, 0));
+    if (int r = decode_device(c, d_in, d_coff, d_clen, d_meth, d_rlen, k, bl, S.out.as<uint8_t>(), d_ooff, d_crc,
                               d_err, st))
       return r;
-    if (raw_total) ZC_CUDA(cudaMemcpyAsync(out + out_at, c->s_out.p, raw_total, cudaMemcpyDeviceToHost, st));
-    ZC_CUDA(cudaMemcpyAsync(h_crc, d_crc, (size_t)k * 8, cudaMemcpyDeviceToHost, st));
-    ZC_CUDA(cudaStreamSynchronize(st));
-    for (uint32_t b = 0; b < k; ++b) {
-      if (crcs_out) crcs_out[b0 + b] = h_crc[b];
-      if (block_err) block_err[b0 + b] = h_err[b];
-      if (h_err[b] && status == ZC_OK) {
-        status = ZC_E_DATA;
-        char m[128];
-        snprintf(m, sizeof m, "block %u damaged (GPU decoder, code %u)", b0 + b, h_err[b]);
-        c->err = m;
-      }
-    }
+    ZC_CUDA(cudaEventRecord(S.ev_done, st));
+    if (have_prev)
+      if (int r = harvest(c->pipe[(it - 1) & 1], prev)) return r;
+    prev = q;
+    have_prev = true;
     out_at += raw_total;
   }
+  if (have_prev)
+    if (int r = harvest(c->pipe[(it - 1) & 1], prev)) return r;
   return status;
 }
 
