@@ -257,12 +257,12 @@ __device__ __forceinline__ uint32_t lcp32(const uint4& a0, const uint4& a1, cons
 // (a warp claims positions for all its idle lanes at once), keeping warps full until the tile drains.
 // A candidate whose byte at the current best length differs from the position's cannot be longer and
 // is skipped after one shared byte load (the CPU parse's probe, src/codec2.h:62).
-// Dynamic shared memory: (tile + depth) * (WB + 4 + 2) bytes.
+// Dynamic shared memory: (tile + depth) * (WB + 4 + 2) + 8 * tile bytes (+4).
 template <uint32_t WB>
 __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   constexpr uint32_t NV = WB / 16;  // uint4s per window
   extern __shared__ uint4 sm[];
-  __shared__ uint32_t next;
+  __shared__ uint32_t next, nwork;
   const uint32_t b = blockIdx.y, t = threadIdx.x, lane = lane_id();
   const uint32_t tile = A.match_tile;
   const uint32_t r0 = blockIdx.x * tile;
@@ -275,12 +275,13 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   uint4* win = sm;  // entry i: bytes 16 v .. 16 v + 15 at win[NV i + v]
   uint32_t* spos = reinterpret_cast<uint32_t*>(win + NV * cap_e);
   uint16_t* sh = reinterpret_cast<uint16_t*>(spos + cap_e);
+  uint32_t* wl = reinterpret_cast<uint32_t*>(sh + ((cap_e + 1) & ~1u));  // work list: entry | best << 16, distance
   const uint8_t* wb = reinterpret_cast<const uint8_t*>(win);
   const uint32_t e0 = r0 > D ? r0 - D : 0, e1 = min(r0 + tile, count);
   const uint64_t base = A.in_off[b];
   const uint32_t* w32 = reinterpret_cast<const uint32_t*>(A.in);
   const uint64_t wend = (base + n + 3) >> 2;  // words at or past it are not read (they lie past the block)
-  if (t == 0) next = 0;
+  if (t == 0) { next = 0; nwork = 0; }
   for (uint32_t i = t; e0 + i < e1; i += 256) {
     const uint32_t r = e0 + i;
     const uint32_t p = A.srt_pos[so + r];
@@ -301,9 +302,37 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   for (uint32_t r = max(r0, count) + t; r < min(r0 + tile, n); r += 256) A.minfo[so + r] = M_NONE;
   __syncthreads();
   const uint32_t tn = e1 > r0 ? e1 - r0 : 0;  // positions of this tile
-  // per-lane scan state: the position's entry li, its chain of kend earlier entries with the same hash
-  // (found by a binary search: the entries are sorted by hash), the candidate k reached so far, the
-  // best length, its distance, and the position's own byte at offset `best` (the probe)
+  // pass 1, a thread per position: the nearest candidate decides most positions (no candidate, a chain
+  // of one, or a match that reaches the cap); the others go to the work list with what it found
+  for (uint32_t my = t; my < tn; my += 256) {
+    const uint32_t r = r0 + my, li = r - e0;
+    const uint32_t p = spos[li], h = sh[li];
+    const uint32_t lim = min(kMaxMatch, n - p), cap = min(min(A.cmp_cap, WB), lim);
+    uint32_t v = M_NONE;
+    if (r > 0 && sh[li - 1] == h) {
+      const uint32_t e = li - 1;
+      const uint32_t l = min(NV == 2 ? lcp32(win[2 * e], win[2 * e + 1], win[2 * li], win[2 * li + 1])
+                                     : lcp16(win[e], win[li]), cap);
+      const uint32_t d = p - spos[e];
+      if (l == cap) {
+        v = cap < lim ? M_SAT | r : m_pack(l, d);
+      } else if (r < 2 || D < 2 || sh[li - 2] != h) {
+        v = l < 4 ? M_NONE : m_pack(l, d);
+      } else {
+        const uint32_t w = atomicAdd(&nwork, 1u);
+        wl[2 * w] = li | (l << 16);
+        wl[2 * w + 1] = d;
+        continue;
+      }
+    }
+    A.minfo[so + p] = v;
+  }
+  __syncthreads();
+  const uint32_t tw = nwork;
+  // pass 2 over the work list, lanes taking entries from a CTA counter.  Per-lane state: the position's
+  // entry li, its chain of kend earlier entries with the same hash (found by a binary search: the
+  // entries are sorted by hash), the candidate k reached so far, the best length, its distance, and the
+  // position's own byte at offset `best` (the probe)
   uint32_t li = 0xFFFFFFFFu, p = 0, lim = 0, cap = 0, best = 0, bd = 0, k = 0, kend = 0, pb = 0;
   uint4 p0 = make_uint4(0, 0, 0, 0), p1 = p0;
   bool dry = false;  // the tile has no unclaimed positions left (warp-uniform)
@@ -315,19 +344,23 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
       uint32_t got = 0;
       if (lane == leader) got = atomicAdd(&next, (uint32_t)__popc(want));
       got = __shfl_sync(kFull, got, leader);
-      if (got + (uint32_t)__popc(want) >= tn) dry = true;
+      if (got + (uint32_t)__popc(want) >= tw) dry = true;
       if (idle) {
         const uint32_t my = got + (uint32_t)__popc(want & ((1u << lane) - 1u));
-        if (my < tn) {
-          const uint32_t r = r0 + my;
-          li = r - e0;
+        if (my < tw) {
+          const uint32_t wa = wl[2 * my];
+          li = wa & 0xFFFFu;
+          best = wa >> 16;
+          bd = wl[2 * my + 1];
+          const uint32_t r = li + e0;
           p = spos[li];
           const uint32_t h = sh[li];
           lim = min(kMaxMatch, n - p);
           cap = min(min(A.cmp_cap, WB), lim);
           p0 = win[NV * li];
           p1 = win[NV * li + NV - 1];
-          best = 0; bd = 0; k = 0; pb = 0;
+          k = 1;
+          pb = wb[WB * li + best];
           uint32_t lo = li - min(D, r), hi = li;  // the first entry of [lo, li] with hash h
           while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
@@ -919,7 +952,9 @@ __global__ void __launch_bounds__(256) k_enc_emit(EncArgs A) {
   for (uint32_t k = i + threadIdx.x; k < len; k += blockDim.x) d[k] = s[k];
 }
 
-size_t match_smem_bytes(uint32_t tile, uint32_t depth, uint32_t wb) { return (size_t)(tile + depth) * (wb + 4 + 2); }
+size_t match_smem_bytes(uint32_t tile, uint32_t depth, uint32_t wb) {
+  return (size_t)(tile + depth) * (wb + 4 + 2) + 4 + (size_t)tile * 8;  // (+ the work list)
+}
 
 cudaError_t prepare_kernels() {  // with the device current, once per context
   cudaError_t e = cudaFuncSetAttribute(k_enc_match<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
