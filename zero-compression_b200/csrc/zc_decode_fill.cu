@@ -2,10 +2,10 @@
 //
 //   k_dec_tokens  one CTA of 1024 threads per block: every token's literal run and match length (ext
 //                 bytes), offset (offset bits), output start and literal start, from block-wide scans, in
-//                 parallel over the tokens; then one warp resolves the recent-offset symbols (they name
-//                 the offsets of the group before, src/codec2.h:180-192) 32 tokens at a time and checks
-//                 the groups.  Every check of the reference decoder is made here; a failing one records a
-//                 status and the block is not replayed.
+//                 parallel over the tokens; then the groups (a scan of their counts) and the recent-offset
+//                 symbols (each names an earlier token's offset, src/codec2.h:180-192), resolved by pointer
+//                 jumping over all tokens at once.  Every check of the reference decoder is made here; a
+//                 failing one records a status and the block is not replayed.
 //   k_dec_fill    one warp per block: walks the groups in order and fills each group's output with all
 //                 lanes (a group's matches read only output from before the group, or their own
 //                 literals), the next 32 tokens' table loaded while the current ones are filled.
@@ -39,11 +39,39 @@ __device__ __forceinline__ uint32_t cta_scan(uint32_t v, uint32_t* ws, uint32_t&
 }
 
 constexpr uint32_t kRepMark = 0x80000000u;  // a recent-offset symbol not resolved yet: kRepMark | index
+constexpr uint32_t kGrpStart = 0x40000000u; // (while groups are scanned) the first token of a group
+
+// inclusive max over the CTA in thread order (blockDim.x == 1024); `total` gets the CTA's max.  ws: 33 words
+__device__ __forceinline__ uint32_t cta_max_incl(uint32_t v, uint32_t* ws, uint32_t& total) {
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, x, o);
+    if (lane >= (uint32_t)o) x = max(x, y);
+  }
+  if (lane == 31) ws[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t z = ws[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(kFull, z, o);
+      if (lane >= (uint32_t)o) z = max(z, y);
+    }
+    ws[lane] = z;  // inclusive over warps
+  }
+  __syncthreads();
+  const uint32_t r = w ? max(x, ws[w - 1]) : x;
+  total = ws[31];
+  __syncthreads();
+  return r;
+}
 
 }  // namespace
 
-__global__ void __launch_bounds__(1024) k_dec_tokens(DecArgs A) {
-  const uint32_t b = blockIdx.x, tid = threadIdx.x, lane = tid & 31u;
+__global__ void __launch_bounds__(1024, 2) k_dec_tokens(DecArgs A) {
+  const uint32_t b = blockIdx.x, tid = threadIdx.x;
   if (A.method[b] != 1 || A.raw_len[b] > A.B || A.err[b]) return;
   __shared__ uint32_t ws[33];
   __shared__ uint32_t any_bad;
@@ -109,69 +137,65 @@ __global__ void __launch_bounds__(1024) k_dec_tokens(DecArgs A) {
   }
   if (bad) any_bad = 1;
   __syncthreads();
-  // ---- recent offsets and groups, one warp, 32 tokens at a time (as the reference decodes them:
-  //      recent = the last three offsets before the group's first token, src/codec2.h:179, 199)
-  if (tid < 32 && !any_bad) {
-    uint32_t l0 = 1, l1 = 4, l2 = 8, r0 = 1, r1 = 4, r2 = 8, gi = 0, gend = 0;
-    bool wbad = false;
-    for (uint32_t t = 0; t < m.nt && !wbad; t += 32) {
-      const uint32_t c = min(32u, m.nt - t);
-      const bool on = lane < c;
-      const uint32_t gk = gi + lane;
-      const uint32_t gcnt = gk < m.ng ? grp[gk] : 0u;
-      const uint32_t gincl = warp_incl_scan(gcnt);
-      const uint32_t gstart = gend + gincl - gcnt;
-      const bool gin = gk < m.ng && gstart < t + c;
-      bool lbad = gin && gcnt == 0;
-      const uint32_t ngc = __popc(__ballot_sync(kFull, gin));
-      const uint32_t mask = __reduce_or_sync(kFull, gin ? 1u << (gstart - t) : 0u);
-      const uint32_t new_gend = ngc ? __shfl_sync(kFull, gstart + gcnt, ngc - 1) : gend;
-      if (new_gend < t + c || new_gend > m.nt) lbad = true;
-      const unsigned below = mask & (0xFFFFFFFFu >> (31u - lane));
-      const int gsl = below ? 31 - __clz(below) : -1;
-      uint32_t D = on ? Td[t + lane] : 1u;
-      const uint32_t ms = on ? Tm[t + lane] : 0xFFFFFFFFu;
-      bool resolved = !(D & kRepMark);
-      int srcl = (int)lane;
-      if (!resolved) {
-        const uint32_t r = D & 3u;
-        if (gsl < 0) { D = r == 0 ? r0 : r == 1 ? r1 : r2; resolved = true; }
-        else if ((int)r >= gsl) {
-          const uint32_t i = r - (uint32_t)gsl;
-          D = i == 0 ? l0 : i == 1 ? l1 : l2;
-          resolved = true;
-        } else {
-          srcl = gsl - 1 - (int)r;
-        }
-      }
-      for (int it = 0; it < 32 && __any_sync(kFull, !resolved); ++it) {
-        const uint32_t v = __shfl_sync(kFull, D, srcl);
-        const bool rv = __shfl_sync(kFull, resolved, srcl);
-        if (!resolved && rv) { D = v; resolved = true; }
-      }
-      if (on && (!resolved || D == 0 || D > ms)) lbad = true;
-      if (on) Td[t + lane] = D;
-      const int gs_last = __shfl_sync(kFull, gsl, c - 1);
-      if (gs_last >= 0) {
-        uint32_t rec[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          const int u = gs_last - 1 - i;
-          const uint32_t v = __shfl_sync(kFull, D, u < 0 ? 0 : u);
-          const int old = -1 - u;
-          rec[i] = u >= 0 ? v : old == 0 ? l0 : old == 1 ? l1 : l2;
-        }
-        r0 = rec[0]; r1 = rec[1]; r2 = rec[2];
-      }
-      for (uint32_t q = c > 3u ? c - 3u : 0u; q < c; ++q) {
-        const uint32_t v = __shfl_sync(kFull, D, q);
-        l2 = l1; l1 = l0; l0 = v;
-      }
-      gi += ngc;
-      gend = new_gend;
-      wbad = __any_sync(kFull, lbad);
+  // ---- groups and recent offsets (src/codec2.h:179-199).  A recent-offset symbol r of a group whose first
+  //      token is gs names the offset of token gs - 1 - r (the last three offsets before the group,
+  //      nearest first), or the initial 1, 4, 8 when r >= gs.  So: group starts (a scan of the group
+  //      counts) flag their first tokens; a max-scan gives each token its group's start; each recent-
+  //      offset token then points at the token it names, and pointer jumping resolves chains of them.
+  __syncthreads();
+  if (!any_bad) {
+    uint32_t gbase = 0;
+    for (uint32_t g0 = 0; g0 < m.ng; g0 += 1024) {
+      const uint32_t g = g0 + tid;
+      const uint32_t c = g < m.ng ? grp[g] : 0u;
+      uint32_t tot;
+      const uint32_t at = gbase + cta_scan(c, ws, tot);
+      if (g < m.ng && (c == 0 || (uint64_t)at + c > m.nt)) bad = true;
+      else if (g < m.ng) Td[at] |= kGrpStart;
+      gbase += tot;
     }
-    if (lane == 0 && (wbad || gend != m.nt || gi != m.ng)) any_bad = 1;
+    if (gbase != m.nt) bad = true;
+  }
+  if (bad) any_bad = 1;
+  __syncthreads();
+  if (!any_bad) {
+    uint32_t carry = 0;
+    for (uint32_t t0 = 0; t0 < m.nt; t0 += 1024) {
+      const uint32_t t = t0 + tid;
+      const bool on = t < m.nt;
+      uint32_t v = on ? Td[t] : 0u;
+      uint32_t tmax;
+      const uint32_t gs = max(carry, cta_max_incl(on && (v & kGrpStart) ? t : 0u, ws, tmax));
+      carry = max(carry, tmax);
+      if (on) {
+        v &= ~kGrpStart;
+        if (v & kRepMark) {
+          const uint32_t r = v & 3u;
+          v = r < gs ? kRepMark | (gs - 1u - r) : (r - gs == 0 ? 1u : r - gs == 1 ? 4u : 8u);
+        }
+        Td[t] = v;
+      }
+    }
+  }
+  __syncthreads();
+  if (!any_bad) {
+    for (int round = 0; round < 32; ++round) {  // (a chain halves each round: at most 20 for 2^20 tokens)
+      bool more = false;
+      for (uint32_t t = tid; t < m.nt; t += 1024) {
+        const uint32_t v = Td[t];
+        if (v & kRepMark) {
+          const uint32_t w = Td[v & ~kRepMark];
+          Td[t] = w;
+          more |= (w & kRepMark) != 0;
+        }
+      }
+      if (!__syncthreads_or(more)) break;
+    }
+    for (uint32_t t = tid; t < m.nt; t += 1024) {
+      const uint32_t D = Td[t];
+      if ((D & kRepMark) || D == 0 || D > Tm[t]) bad = true;
+    }
+    if (bad) any_bad = 1;
   }
   __syncthreads();
   if (tid == 0) {

@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(256) k_sort_scan(EncArgs A) {
 }
 
 template <int PASS>
-__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(EncArgs A) {
+__global__ void __launch_bounds__(kSortThreads, 4) k_sort_scatter(EncArgs A) {
   constexpr uint32_t NW = kSortThreads / 32;
   __shared__ uint32_t cw[NW][256];  // per-warp digit counts, then the warp's start within the digit
   __shared__ uint32_t st_pos[kSortTile];
@@ -524,7 +524,7 @@ __device__ __forceinline__ uint32_t warp_step(const ParseBlock& P, uint32_t p, b
 // chain before it leaves, until that walk meets the previous one (a two-pointer merge), and rounds end
 // when no segment's exit moves.  Then every segment counts and writes its tokens.  Each warp's 32 walks
 // step together (warp_step), so capped matches are finished by whole warps.
-__global__ void __launch_bounds__(256) k_enc_parse(EncArgs A) {
+__global__ void __launch_bounds__(256, 8) k_enc_parse(EncArgs A) {  // (8 CTAs an SM: latency-bound walks)
   const uint32_t b = blockIdx.x, q = threadIdx.x;
   const uint32_t n = A.in_len[b];
   const size_t so = (size_t)b * A.B;
