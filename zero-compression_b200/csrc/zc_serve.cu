@@ -67,6 +67,7 @@ struct Job {
   uint64_t pay_at = 0;                              // compress: next free byte of the job's payload buffer
   uint64_t raw_total = 0;
   cudaEvent_t up = nullptr;                         // recorded after the job's upload
+  bool uploaded = false;                            // its upload is queued and `up` recorded
 };
 
 // a batch's class: the kind of kernels, block size and level it shares
@@ -117,6 +118,11 @@ struct zc_server {
   uint64_t next_id = 1;
   bool stop = false;
   std::thread worker;
+  std::thread uploader;              // uploads admitted jobs' bytes (pageable copies block their caller)
+  std::deque<Job*> upq;
+  std::condition_variable cv_up;
+  bool worker_done = false;          // the uploader outlives the worker (its jobs may still need uploads)
+  bool admit_blocked = false;        // the oldest pending job does not fit until some job finishes
   uint64_t jobs_done = 0, raw_bytes = 0, ticks = 0;
   Slot slot[2];
   int failed = 0;  // a device failure ends the server: every job gets ZC_E_DEVICE
@@ -128,17 +134,38 @@ uint32_t batch_cap(const zc_server* S, uint32_t bl) {
   return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(kCap, S->max_batch >> bl));
 }
 
-// places a job in the arena and starts its upload on the upload stream; false when it does not fit now
+// places a job in the arena and hands it to the uploader; false when it does not fit now
 bool admit(zc_server* S, Job* J) {
   uint64_t off;
   if (!S->arena.alloc(J->footprint, off)) return false;
   J->in_off = off;
   J->out_off = off + Arena::round(J->j.in_len + 64);
   J->admitted = true;
-  if (J->j.in_len) cudaMemcpyAsync(S->arena.base + J->in_off, J->j.in, J->j.in_len, cudaMemcpyHostToDevice, S->ust);
-  cudaMemsetAsync(S->arena.base + J->in_off + J->j.in_len, 0, 64, S->ust);
-  if (cudaEventCreateWithFlags(&J->up, cudaEventDisableTiming) == cudaSuccess) cudaEventRecord(J->up, S->ust);
+  S->upq.push_back(J);
+  S->cv_up.notify_one();
   return true;
+}
+
+// the uploader thread: each admitted job's bytes to its arena range on the upload stream, then the event
+// the kernel stream waits on; the job becomes batchable once the event is recorded
+void uploader(zc_server* S) {
+  cudaSetDevice(S->device);
+  std::unique_lock<std::mutex> lk(S->mu);
+  for (;;) {
+    S->cv_up.wait(lk, [&] { return S->worker_done || !S->upq.empty(); });
+    if (S->upq.empty()) return;  // (the worker has ended)
+    Job* J = S->upq.front();
+    S->upq.pop_front();
+    lk.unlock();
+    if (J->j.in_len) cudaMemcpyAsync(S->arena.base + J->in_off, J->j.in, J->j.in_len, cudaMemcpyHostToDevice, S->ust);
+    cudaMemsetAsync(S->arena.base + J->in_off + J->j.in_len, 0, 64, S->ust);
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) cudaEventRecord(ev, S->ust);
+    lk.lock();
+    J->up = ev;
+    J->uploaded = true;
+    S->cv_work.notify_all();
+  }
 }
 
 void finish(zc_server* S, Job* J, int status) {
@@ -146,7 +173,10 @@ void finish(zc_server* S, Job* J, int status) {
   if (status && !J->status) J->status = status;
   J->done = true;
   J->t_done = now_s();
-  if (J->admitted) S->arena.release(J->in_off, J->footprint);
+  if (J->admitted) {
+    S->arena.release(J->in_off, J->footprint);
+    S->admit_blocked = false;
+  }
   if (J->up) { cudaEventDestroy(J->up); J->up = nullptr; }
   S->jobs_done += 1;
   S->raw_bytes += J->raw_total;
@@ -303,7 +333,7 @@ void complete_batch(zc_server* S, Slot& L) {
 void finish_done(zc_server* S) {
   for (auto it = S->active.begin(); it != S->active.end();) {
     Job* J = *it;
-    if (J->finished == J->nb && J->next == J->nb) { finish(S, J, ZC_OK); it = S->active.erase(it); }
+    if (J->uploaded && J->finished == J->nb && J->next == J->nb) { finish(S, J, ZC_OK); it = S->active.erase(it); }
     else ++it;
   }
   S->cv_done.notify_all();
@@ -311,15 +341,23 @@ void finish_done(zc_server* S) {
 
 // Each pass queues the next batch in one slot, then finishes the batch queued in the other slot on the
 // pass before: the GPU runs batch k + 1 while the host hands out batch k's results.
+void worker_loop(zc_server* S, std::unique_lock<std::mutex>& lk);
+
 void worker(zc_server* S) {
   cudaSetDevice(S->device);
   std::unique_lock<std::mutex> lk(S->mu);
+  worker_loop(S, lk);
+  S->worker_done = true;
+  S->cv_up.notify_all();
+}
+
+void worker_loop(zc_server* S, std::unique_lock<std::mutex>& lk) {
   int cur = 0;  // the slot the next batch goes to
   for (;;) {
     const bool inflight = S->slot[0].busy || S->slot[1].busy;
     S->cv_work.wait(lk, [&] {
-      if (inflight || !S->pending.empty() || S->failed) return true;
-      for (Job* J : S->active) if (J->next < J->nb || J->finished == J->nb) return true;
+      if (inflight || (!S->pending.empty() && !S->admit_blocked) || S->failed) return true;
+      for (Job* J : S->active) if (J->uploaded && (J->next < J->nb || J->finished == J->nb)) return true;
       return S->stop && S->active.empty();
     });
     if (S->stop && S->pending.empty() && S->active.empty() && !inflight) return;
@@ -327,6 +365,7 @@ void worker(zc_server* S) {
       for (Slot& L : S->slot) if (L.busy) { lk.unlock(); complete_batch(S, L); lk.lock(); }
       for (Job* J : S->active) finish(S, J, S->failed);
       for (Job* J : S->pending) finish(S, J, S->failed);
+      S->upq.clear();
       S->active.clear();
       S->pending.clear();
       S->cv_done.notify_all();
@@ -335,7 +374,8 @@ void worker(zc_server* S) {
       continue;
     }
     // admission in arrival order, while the arena has room
-    while (!S->pending.empty() && admit(S, S->pending.front())) {
+    while (!S->pending.empty() && !S->admit_blocked) {
+      if (!admit(S, S->pending.front())) { S->admit_blocked = true; break; }
       S->active.push_back(S->pending.front());
       S->pending.pop_front();
     }
@@ -343,7 +383,7 @@ void worker(zc_server* S) {
     bool queued = false;
     Slot& L = S->slot[cur];
     Job* first = nullptr;
-    for (Job* J : S->active) if (J->next < J->nb) { first = J; break; }
+    for (Job* J : S->active) if (J->uploaded && J->next < J->nb) { first = J; break; }
     if (first && !L.busy) {
       const Cls k = cls_of(first);
       const uint32_t cap = batch_cap(S, k.bl);
@@ -351,7 +391,7 @@ void worker(zc_server* S) {
       L.take.clear();
       uint64_t bytes = 0;
       for (Job* J : S->active) {
-        if (!(cls_of(J) == k)) continue;
+        if (!J->uploaded || !(cls_of(J) == k)) continue;
         while (J->next < J->nb && L.take.size() < cap) {
           const uint64_t nbytes = (uint64_t)(k.compress ? J->blen[J->next] : J->rlen[J->next]);
           if (!L.take.empty() && bytes + nbytes > S->max_batch) break;
@@ -417,6 +457,7 @@ int zc_serve_open(zc_server** out, int device, uint64_t budget_bytes, uint64_t m
     return e == cudaErrorMemoryAllocation ? ZC_E_NOMEM : (rc ? rc : ZC_E_DEVICE);
   }
   S->worker = std::thread(worker, S);
+  S->uploader = std::thread(uploader, S);
   *out = S;
   return ZC_OK;
 }
@@ -429,7 +470,12 @@ void zc_serve_close(zc_server* S) {
       S->stop = true;
     }
     S->cv_work.notify_all();
+    S->cv_up.notify_all();
     S->worker.join();
+  }
+  if (S->uploader.joinable()) {
+    S->cv_up.notify_all();
+    S->uploader.join();
   }
   cudaSetDevice(S->device);
   for (cudaStream_t x : {S->st, S->ust, S->cst})
