@@ -638,6 +638,15 @@ def run_decode(args):
     return 0 if ok else 1
 
 
+def pinned_copy(a):
+    """(numpy view, owning tensor) of a page-locked copy of u8 array a."""
+    import torch
+    t = torch.empty(max(a.size, 1), dtype=torch.uint8, pin_memory=True)
+    v = t.numpy()[:a.size]
+    v[:] = a
+    return v, t
+
+
 def run_serve(args):
     """The serving workload: an open-loop Poisson stream of jobs (60 % compress, 30 % extract, 10 % test),
     each one file of log-uniform size from the many-file generator mix, block size from {16, 18, 20}, level
@@ -661,9 +670,11 @@ def run_serve(args):
             data = G.by_kind(int(kinds[i]), int(sizes[i]), bl, 8000 + i)
             meth, lens, crcs, pay, offs = codec.compress_arrays(data, bl, level=lv)
             blob, clens, rlens = Z.record_bodies(data, meth, lens, pay, offs, bl)
-            pool.append(dict(data=data, bl=bl, lv=lv, blob=blob, clens=clens, meth=meth.copy(), rlens=rlens,
-                             crcs=crcs.copy()))
-    srv = Z.Server(budget_bytes=args.budget_gib << 30, device=local)
+            # the clients' buffers are page-locked, as a server's I/O buffers would be
+            pdata, pblob = pinned_copy(data), pinned_copy(blob)
+            pool.append(dict(data=pdata[0], bl=bl, lv=lv, blob=pblob[0], clens=clens, meth=meth.copy(), rlens=rlens,
+                             crcs=crcs.copy(), keep=(pdata[1], pblob[1])))
+    srv = Z.Server(budget_bytes=args.budget_gib << 30, device=local, pinned=True)
     rates = [float(r) for r in args.rates.split(",")]
     results = []
     for rate in rates:
@@ -716,7 +727,9 @@ def run_serve(args):
                         "p50_ms": round(float(np.percentile(lat_ms, 50)), 2) if njobs else None,
                         "p99_ms": round(float(np.percentile(lat_ms, 99)), 2) if njobs else None,
                         "ticks": s1["ticks"] - s0["ticks"], "errors": int(sum(1 for x in statuses if x)),
-                        "wall_s": round(wall, 2)})
+                        "wall_s": round(wall, 2),
+                        "gpu_busy": round((s1["gpu_s"] - s0["gpu_s"]) / wall, 3),
+                        "worker_s": {k: round(s1[k] - s0[k], 3) for k in ("wait_s", "handout_s", "upload_s")}})
         print(json.dumps({"serve_rate": results[-1]}), file=sys.stderr, flush=True)
         if wall > args.duration * 2.0:  # saturated: the backlog took as long again as the arrivals
             break

@@ -134,6 +134,11 @@ int zc_decompress_noalloc(const uint8_t *d_comp, const uint64_t *d_comp_offs, co
  * and when turned off. */
 int zc_set_graphs(zc_ctx *ctx, int on);
 
+/* Sizes the context's device scratch now for device calls of up to nb blocks of 2^block_log bytes, in both
+ * directions (no reference counterpart).  Scratch is kept by capacity, so later calls that fit, of any
+ * block size, allocate nothing and keep their captured graphs. */
+int zc_reserve(zc_ctx *ctx, uint32_t block_log, uint32_t nb);
+
 /* ---- launch shapes and the autotuner (no reference counterpart: the reference's kernels have fixed
  * work-group sizes, kernels/zero.cl).  A shape is kept per (block_log, level class: level 1, 2..8, 9)
  * and never changes a result byte, only speed:
@@ -197,8 +202,14 @@ typedef struct zc_server zc_server;
 int zc_serve_open(zc_server **srv, int device, uint64_t budget_bytes, uint64_t max_batch_bytes);
 /* Waits for every submitted job, then stops the worker and frees the device memory. */
 void zc_serve_close(zc_server *srv);
-/* Queues a job; *id identifies it.  ZC_E_ARG when it could never fit the budget. */
+/* Queues a job; *id identifies it.  ZC_E_ARG when it could never fit the budget.  The job's buffers must
+ * stay valid until zc_serve_wait returns.  Page-locked buffers are faster: the input is uploaded without
+ * staging, and an extract job's page-locked `out` receives its bytes by DMA, with no host copy. */
 int zc_serve_submit(zc_server *srv, const zc_job *job, uint64_t *id);
+/* Seconds accumulated since open: the GPU time of the batches' kernels (CUDA events around each batch's
+ * graph), the worker's waits for batches in flight, its hand-out of results to jobs, and the uploader's
+ * time in job uploads.  GPU time over wall time is the device's busy fraction. */
+int zc_serve_times(zc_server *srv, double *gpu_s, double *wait_s, double *handout_s, double *upload_s);
 /* Waits for job `id`; returns its status (ZC_OK, ZC_E_DATA for a damaged block, ...) and, when
  * latency_s is not NULL, the seconds from its submission to its completion. */
 int zc_serve_wait(zc_server *srv, uint64_t id, double *latency_s);

@@ -129,12 +129,10 @@ struct zc_ctx {
   zc::Stages stages;
   StageRecords records;
   zc::CrcTables* d_crct = nullptr;
-  // encoder scratch for enc_nb blocks of 2^enc_bl bytes
-  uint32_t enc_nb = 0, enc_bl = 0;
+  // encoder scratch (sized by capacity: any block size whose blocks fit)
   DevBuf e_tmp_pos, e_srt_pos, e_minfo, e_scnt, e_tk_seg, e_tmp_h, e_srt_h, e_tk_i, e_tk_m, e_tk_d, e_bcnt, e_lit, e_tok,
       e_ext, e_sym, e_grp, e_bits, e_lanes, e_freq, e_lanelen, e_sinfo, e_slab;
-  // decoder scratch for dec_nb blocks of 2^dec_bl bytes
-  uint32_t dec_nb = 0, dec_bl = 0;
+  // decoder scratch (likewise)
   DevBuf d_lit, d_tok, d_sym, d_grp, d_ext, d_meta, d_tks, d_tkm, d_tkd, d_tkl, d_tot;
   // staging for the host-pointer calls
   DevBuf s_in, s_blk, s_out, s_meta;
@@ -195,56 +193,46 @@ void drop_graphs(zc_ctx* c) {
   c->graph_cache.clear();
 }
 
-int ensure_enc(zc_ctx* c, uint32_t nb, uint32_t block_log) {
-  if (nb <= c->enc_nb && block_log == c->enc_bl) return ZC_OK;
-  drop_graphs(c);  // (captured graphs name the scratch being replaced)
-  const size_t B = (size_t)1 << block_log, TC = zc::tok_cap((uint32_t)B), EC = zc::ext_cap((uint32_t)B);
-  const size_t N = (size_t)nb * B;
-  ZC_CUDA(grow(c->e_tmp_pos, N * 4));
-  ZC_CUDA(grow(c->e_srt_pos, N * 4));
-  ZC_CUDA(grow(c->e_minfo, N * 4));
-  ZC_CUDA(grow(c->e_scnt, (size_t)nb * ((B + 4095) / 4096) * 256 * 4));
-  ZC_CUDA(grow(c->e_tk_seg, (size_t)nb * 3 * zc::seg_tok_cap((uint32_t)B) * 4));
-  ZC_CUDA(grow(c->e_tmp_h, N * 2));
-  ZC_CUDA(grow(c->e_srt_h, N * 2));
-  ZC_CUDA(grow(c->e_tk_i, nb * TC * 4));
-  ZC_CUDA(grow(c->e_tk_m, nb * TC * 4));
-  ZC_CUDA(grow(c->e_tk_d, nb * TC * 4));
-  ZC_CUDA(grow(c->e_bcnt, (size_t)nb * 8 * 4));
-  ZC_CUDA(grow(c->e_lit, N));
-  ZC_CUDA(grow(c->e_tok, nb * TC));
-  ZC_CUDA(grow(c->e_ext, nb * EC));
-  ZC_CUDA(grow(c->e_sym, nb * TC));
-  ZC_CUDA(grow(c->e_grp, nb * TC));
-  ZC_CUDA(grow(c->e_bits, (size_t)nb * zc::bits_cap((uint32_t)B)));
-  ZC_CUDA(grow(c->e_lanes, (size_t)nb * zc::lanes_per_block((uint32_t)B)));
-  ZC_CUDA(grow(c->e_freq, (size_t)nb * 5 * 256 * 2));
-  ZC_CUDA(grow(c->e_lanelen, (size_t)nb * 5 * 64 * 4));
-  ZC_CUDA(grow(c->e_sinfo, (size_t)nb * 5 * 4 * 4));
-  ZC_CUDA(grow(c->e_slab, N));
-  c->enc_nb = nb;
-  c->enc_bl = block_log;
+// Scratch is sized by capacity: a call whose buffers already fit (any block size) changes nothing and
+// keeps the captured graphs; a call that needs more drops them (they name the buffers being replaced).
+struct Need {
+  DevBuf* b;
+  size_t bytes;
+};
+template <size_t K>
+int ensure(zc_ctx* c, Need (&need)[K]) {
+  bool grows = false;
+  for (const Need& x : need) grows |= !x.b->p || x.bytes > x.b->n;
+  if (!grows) return ZC_OK;
+  drop_graphs(c);
+  for (const Need& x : need) ZC_CUDA(grow(*x.b, x.bytes));
   return ZC_OK;
 }
 
-int ensure_dec(zc_ctx* c, uint32_t nb, uint32_t block_log) {
-  if (nb <= c->dec_nb && block_log == c->dec_bl) return ZC_OK;
-  drop_graphs(c);
+int ensure_enc(zc_ctx* c, uint32_t nb, uint32_t block_log) {
   const size_t B = (size_t)1 << block_log, TC = zc::tok_cap((uint32_t)B), EC = zc::ext_cap((uint32_t)B);
-  ZC_CUDA(grow(c->d_lit, (size_t)nb * B));
-  ZC_CUDA(grow(c->d_tok, (size_t)nb * TC));
-  ZC_CUDA(grow(c->d_sym, (size_t)nb * TC));
-  ZC_CUDA(grow(c->d_grp, (size_t)nb * TC));
-  ZC_CUDA(grow(c->d_ext, (size_t)nb * EC));
-  ZC_CUDA(grow(c->d_meta, (size_t)nb * sizeof(zc::DecMeta)));
-  ZC_CUDA(grow(c->d_tks, (size_t)nb * TC * 4));
-  ZC_CUDA(grow(c->d_tkm, (size_t)nb * TC * 4));
-  ZC_CUDA(grow(c->d_tkd, (size_t)nb * TC * 4));
-  ZC_CUDA(grow(c->d_tkl, (size_t)nb * TC * 4));
-  ZC_CUDA(grow(c->d_tot, (size_t)nb * 8));
-  c->dec_nb = nb;
-  c->dec_bl = block_log;
-  return ZC_OK;
+  const size_t N = (size_t)nb * B;
+  Need need[] = {
+      {&c->e_tmp_pos, N * 4}, {&c->e_srt_pos, N * 4}, {&c->e_minfo, N * 4},
+      {&c->e_scnt, (size_t)nb * ((B + 4095) / 4096) * 256 * 4},
+      {&c->e_tk_seg, (size_t)nb * 3 * zc::seg_tok_cap((uint32_t)B) * 4},
+      {&c->e_tmp_h, N * 2}, {&c->e_srt_h, N * 2},
+      {&c->e_tk_i, nb * TC * 4}, {&c->e_tk_m, nb * TC * 4}, {&c->e_tk_d, nb * TC * 4},
+      {&c->e_bcnt, (size_t)nb * 8 * 4}, {&c->e_lit, N}, {&c->e_tok, nb * TC}, {&c->e_ext, nb * EC},
+      {&c->e_sym, nb * TC}, {&c->e_grp, nb * TC}, {&c->e_bits, (size_t)nb * zc::bits_cap((uint32_t)B)},
+      {&c->e_lanes, (size_t)nb * zc::lanes_per_block((uint32_t)B)}, {&c->e_freq, (size_t)nb * 5 * 256 * 2},
+      {&c->e_lanelen, (size_t)nb * 5 * 64 * 4}, {&c->e_sinfo, (size_t)nb * 5 * 4 * 4}, {&c->e_slab, N}};
+  return ensure(c, need);
+}
+
+int ensure_dec(zc_ctx* c, uint32_t nb, uint32_t block_log) {
+  const size_t B = (size_t)1 << block_log, TC = zc::tok_cap((uint32_t)B), EC = zc::ext_cap((uint32_t)B);
+  Need need[] = {
+      {&c->d_lit, (size_t)nb * B}, {&c->d_tok, (size_t)nb * TC}, {&c->d_sym, (size_t)nb * TC},
+      {&c->d_grp, (size_t)nb * TC}, {&c->d_ext, (size_t)nb * EC}, {&c->d_meta, (size_t)nb * sizeof(zc::DecMeta)},
+      {&c->d_tks, (size_t)nb * TC * 4}, {&c->d_tkm, (size_t)nb * TC * 4}, {&c->d_tkd, (size_t)nb * TC * 4},
+      {&c->d_tkl, (size_t)nb * TC * 4}, {&c->d_tot, (size_t)nb * 8}};
+  return ensure(c, need);
 }
 
 bool bad_block_log(uint32_t bl) { return bl < zc::kMinBlockLog || bl > zc::kMaxBlockLog; }
@@ -571,6 +559,16 @@ int zc_prepare(zc_ctx* c, uint32_t block_log, int level) {
   c->block_log = block_log;
   c->level = level;
   return ZC_OK;
+}
+
+int zc_reserve(zc_ctx* c, uint32_t block_log, uint32_t nb) {
+  if (!c) return ZC_E_ARG;
+  if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  if (nb > enc_blocks_per_launch(block_log) || nb > dec_blocks_per_launch(block_log))
+    return fail(c, ZC_E_ARG, "too many blocks for one launch");
+  ZC_CUDA(cudaSetDevice(c->device));
+  if (int r = ensure_enc(c, std::max(nb, 1u), block_log)) return r;
+  return ensure_dec(c, std::max(nb, 1u), block_log);
 }
 
 size_t zc_batch_bytes(const zc_ctx*, uint32_t block_log) { return (size_t)enc_blocks_per_launch(block_log) << block_log; }

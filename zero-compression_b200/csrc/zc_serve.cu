@@ -68,6 +68,7 @@ struct Job {
   uint64_t raw_total = 0;
   cudaEvent_t up = nullptr;                         // recorded after the job's upload
   bool uploaded = false;                            // its upload is queued and `up` recorded
+  bool out_pinned = false;                          // extract: `out` is page-locked (copied into directly)
 };
 
 // a batch's class: the kind of kernels, block size and level it shares
@@ -95,6 +96,7 @@ struct Slot {
   uint8_t* h = nullptr;        // pinned: descriptors up, results down
   uint8_t* h_stage = nullptr;  // pinned: payloads (compress) or raw bytes (extract) down
   cudaEvent_t ev = nullptr;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;  // timing: around the batch's graph
   bool busy = false;
   Cls k{};
   std::vector<std::pair<Job*, uint32_t>> take;
@@ -110,7 +112,7 @@ struct zc_server {
   cudaStream_t cst = nullptr;  // payload copies of a finished batch, beside the next batch's kernels
   Arena arena;
   uint64_t max_batch = 256ull << 20;
-  std::mutex mu;
+  std::mutex mu, tmu;  // (tmu: the timing totals)
   std::condition_variable cv_work, cv_done;
   std::deque<Job*> pending;
   std::vector<Job*> active;
@@ -124,6 +126,7 @@ struct zc_server {
   bool worker_done = false;          // the uploader outlives the worker (its jobs may still need uploads)
   bool admit_blocked = false;        // the oldest pending job does not fit until some job finishes
   uint64_t jobs_done = 0, raw_bytes = 0, ticks = 0;
+  double gpu_s = 0, wait_s = 0, handout_s = 0, upload_s = 0;  // accumulated (zc_serve_times)
   Slot slot[2];
   int failed = 0;  // a device failure ends the server: every job gets ZC_E_DEVICE
 };
@@ -157,10 +160,15 @@ void uploader(zc_server* S) {
     Job* J = S->upq.front();
     S->upq.pop_front();
     lk.unlock();
+    const double u0 = now_s();
     if (J->j.in_len) cudaMemcpyAsync(S->arena.base + J->in_off, J->j.in, J->j.in_len, cudaMemcpyHostToDevice, S->ust);
     cudaMemsetAsync(S->arena.base + J->in_off + J->j.in_len, 0, 64, S->ust);
     cudaEvent_t ev = nullptr;
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) cudaEventRecord(ev, S->ust);
+    {
+      std::lock_guard<std::mutex> g(S->tmu);
+      S->upload_s += now_s() - u0;
+    }
     lk.lock();
     J->up = ev;
     J->uploaded = true;
@@ -213,9 +221,13 @@ Views views(Slot& L) {
 // returns without waiting
 void enqueue_batch(zc_server* S, Slot& L) {
   const Cls& k = L.k;
-  const uint32_t cap = batch_cap(S, k.bl);
   Views v = views(L);
   const uint32_t n = (uint32_t)L.take.size();
+  // padded to the next power of two (at least 16, at most the class's capacity): one graph per class and
+  // size bucket, and a small tick does not launch the CTAs of a full one
+  uint32_t cap = 16;
+  while (cap < n) cap <<= 1;
+  cap = std::min(cap, batch_cap(S, k.bl));
   for (uint32_t i = 0; i < cap; ++i) {
     if (i < n) {
       Job* J = L.take[i].first;
@@ -240,9 +252,11 @@ void enqueue_batch(zc_server* S, Slot& L) {
   cudaMemcpyAsync(L.d_a32, v.h1, cap * 4, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(L.d_b32, v.h2, cap * 4, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(L.d_meth, v.hm, cap, cudaMemcpyHostToDevice, st);
+  cudaEventRecord(L.t0, st);
   if (k.compress) {
     L.rc = zc_compress_device(S->ctx, S->arena.base, L.d_a64, L.d_a32, cap, k.bl, k.level, L.d_meth, L.d_c32,
                               L.d_err, L.d_stage, S->max_batch + 64, L.d_b64, L.d_total, st);
+    cudaEventRecord(L.t1, st);
     if (!L.rc) {
       cudaMemcpyAsync(v.r_off, L.d_b64, cap * 8, cudaMemcpyDeviceToHost, st);
       cudaMemcpyAsync(v.r_len, L.d_c32, cap * 4, cudaMemcpyDeviceToHost, st);
@@ -253,6 +267,7 @@ void enqueue_batch(zc_server* S, Slot& L) {
   } else {
     L.rc = zc_decompress_device(S->ctx, S->arena.base, L.d_a64, L.d_a32, L.d_meth, L.d_b32, cap, k.bl,
                                 S->arena.base, L.d_b64, L.d_c32, L.d_err, st);
+    cudaEventRecord(L.t1, st);
     if (!L.rc) {
       cudaMemcpyAsync(v.r_crc, L.d_c32, cap * 4, cudaMemcpyDeviceToHost, st);
       cudaMemcpyAsync(v.r_err, L.d_err, cap * 4, cudaMemcpyDeviceToHost, st);
@@ -267,7 +282,12 @@ void enqueue_batch(zc_server* S, Slot& L) {
           const uint32_t b0 = L.take[i].second, b1 = L.take[e - 1].second;
           const uint64_t o0 = J->bout[b0], o1 = J->bout[b1] + J->rlen[b1];
           len = o1 > o0 ? o1 - o0 : 0;
-          if (len) cudaMemcpyAsync(L.h_stage + at, S->arena.base + J->out_off + o0, len, cudaMemcpyDeviceToHost, st);
+          if (len && J->out_pinned) {  // straight into the caller's page-locked buffer: nothing to hand out
+            cudaMemcpyAsync(J->j.out + o0, S->arena.base + J->out_off + o0, len, cudaMemcpyDeviceToHost, st);
+            len = 0;
+          } else if (len) {
+            cudaMemcpyAsync(L.h_stage + at, S->arena.base + J->out_off + o0, len, cudaMemcpyDeviceToHost, st);
+          }
         }
         L.runs.emplace_back(at, len);
         at += len;
@@ -286,7 +306,11 @@ void complete_batch(zc_server* S, Slot& L) {
   Views v = views(L);
   const uint32_t n = (uint32_t)L.take.size();
   int rc = L.rc;
+  const double w0 = now_s();
   if (!rc && cudaEventSynchronize(L.ev) != cudaSuccess) rc = ZC_E_DEVICE;
+  const double w1 = now_s();
+  float gms = 0;
+  if (!rc) cudaEventElapsedTime(&gms, L.t0, L.t1);
   if (k.compress) {
     if (!rc && *v.r_total) {
       cudaMemcpyAsync(L.h_stage, L.d_stage, *v.r_total, cudaMemcpyDeviceToHost, S->cst);
@@ -328,6 +352,11 @@ void complete_batch(zc_server* S, Slot& L) {
   for (uint32_t i = 0; i < n; ++i) L.take[i].first->finished += 1;
   L.busy = false;
   L.take.clear();
+  const double w2 = now_s();
+  std::lock_guard<std::mutex> g(S->tmu);
+  S->gpu_s += gms * 1e-3;
+  S->wait_s += w1 - w0;
+  S->handout_s += w2 - w1;
 }
 
 void finish_done(zc_server* S) {
@@ -450,8 +479,12 @@ int zc_serve_open(zc_server** out, int device, uint64_t budget_bytes, uint64_t m
     if (e == cudaSuccess) e = cudaMallocHost(&L.h, kCap * 64 + 64);
     if (e == cudaSuccess) e = cudaMallocHost(&L.h_stage, S->max_batch + 64);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreate(&L.t0);
+    if (e == cudaSuccess) e = cudaEventCreate(&L.t1);
   }
   if (e == cudaSuccess) rc = zc_set_graphs(S->ctx, 1);
+  // the codec's scratch for the largest batch of every block size, once: ticks then never reallocate it
+  for (uint32_t bl = 16; bl <= 20 && e == cudaSuccess && !rc; ++bl) rc = zc_reserve(S->ctx, bl, batch_cap(S, bl));
   if (e != cudaSuccess || rc) {
     zc_serve_close(S);
     return e == cudaErrorMemoryAllocation ? ZC_E_NOMEM : (rc ? rc : ZC_E_DEVICE);
@@ -492,6 +525,8 @@ void zc_serve_close(zc_server* S) {
     if (L.h) cudaFreeHost(L.h);
     if (L.h_stage) cudaFreeHost(L.h_stage);
     if (L.ev) cudaEventDestroy(L.ev);
+    if (L.t0) cudaEventDestroy(L.t0);
+    if (L.t1) cudaEventDestroy(L.t1);
   }
   for (cudaStream_t x : {S->st, S->ust, S->cst})
     if (x) cudaStreamDestroy(x);
@@ -536,6 +571,11 @@ int zc_serve_submit(zc_server* S, const zc_job* job, uint64_t* id) {
     if (ci > j.in_len || (j.kind == ZC_JOB_EXTRACT && ro && (!j.out || j.out_cap < ro))) { delete J; return ZC_E_ARG; }
     J->raw_total = ro;
     J->footprint = Arena::round(j.in_len + 64) + Arena::round(ro + 64);
+    if (j.kind == ZC_JOB_EXTRACT && j.out) {
+      cudaPointerAttributes pa;
+      if (cudaPointerGetAttributes(&pa, j.out) == cudaSuccess) J->out_pinned = pa.type == cudaMemoryTypeHost;
+      else cudaGetLastError();
+    }
   } else {
     delete J;
     return ZC_E_ARG;
@@ -574,6 +614,16 @@ int zc_serve_stats(zc_server* S, uint64_t* jobs_done, uint64_t* raw_bytes, uint6
   if (raw_bytes) *raw_bytes = S->raw_bytes;
   if (ticks) *ticks = S->ticks;
   if (arena_used) *arena_used = S->arena.used;
+  return ZC_OK;
+}
+
+int zc_serve_times(zc_server* S, double* gpu_s, double* wait_s, double* handout_s, double* upload_s) {
+  if (!S) return ZC_E_ARG;
+  std::lock_guard<std::mutex> g(S->tmu);
+  if (gpu_s) *gpu_s = S->gpu_s;
+  if (wait_s) *wait_s = S->wait_s;
+  if (handout_s) *handout_s = S->handout_s;
+  if (upload_s) *upload_s = S->upload_s;
   return ZC_OK;
 }
 

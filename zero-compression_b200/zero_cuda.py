@@ -365,15 +365,20 @@ class ServeJob:
 
 class Server:
     """Continuous-batching request loop on one GPU: jobs admitted by free device memory (budget_bytes),
-    their blocks batched with other jobs' blocks tick by tick."""
+    their blocks batched with other jobs' blocks tick by tick.  pinned=True takes the jobs' result
+    buffers from recycled page-locked memory (an extract job's bytes then arrive by DMA, with no host
+    copy); such results are valid while their job handle lives, and the buffers are reused after."""
 
-    def __init__(self, budget_bytes, device=0, max_batch_bytes=0):
+    def __init__(self, budget_bytes, device=0, max_batch_bytes=0, pinned=False):
+        self.pinned = pinned
+        self._free = {}  # pinned result buffers by size class, reused once their job handle is gone
         L = lib()
         L.zc_serve_open.argtypes = [C.POINTER(_vp), C.c_int, C.c_uint64, C.c_uint64]
         L.zc_serve_close.argtypes = [_vp]
         L.zc_serve_submit.argtypes = [_vp, C.POINTER(_Job), C.POINTER(C.c_uint64)]
         L.zc_serve_wait.argtypes = [_vp, C.c_uint64, C.POINTER(C.c_double)]
         L.zc_serve_stats.argtypes = [_vp] + [C.POINTER(C.c_uint64)] * 4
+        L.zc_serve_times.argtypes = [_vp] + [C.POINTER(C.c_double)] * 4
         self._srv = _vp()
         rc = L.zc_serve_open(C.byref(self._srv), device, budget_bytes, max_batch_bytes)
         if rc:
@@ -391,6 +396,24 @@ class Server:
         except Exception:
             pass
 
+    def _buf(self, n, arr, key):
+        if not self.pinned:
+            return np.empty(n, np.uint8)
+        import torch
+        cls = max(1 << 16, 1 << (int(n) - 1).bit_length())
+        free = self._free.setdefault(cls, [])
+        t = free.pop() if free else torch.empty(cls, dtype=torch.uint8, pin_memory=True)
+        arr.setdefault("_pinned", []).append((cls, t))
+        return t.numpy()[:n]
+
+    def _track(self, handle):
+        """Pinned buffers go back to the free lists when the handle is collected."""
+        import weakref
+        for cls, t in handle.arrays.get("_pinned", []):
+            weakref.finalize(handle, self._free.setdefault(cls, []).append, t)
+        handle.arrays.pop("_pinned", None)
+        return handle
+
     def _submit(self, job, handle):
         jid = C.c_uint64()
         rc = lib().zc_serve_submit(self._srv, C.byref(job), C.byref(jid))
@@ -403,14 +426,15 @@ class Server:
         a = _as_u8(data)
         B = 1 << block_log
         nb = (a.size + B - 1) // B
-        arr = dict(data=a, payloads=np.empty(max(a.size, 1), np.uint8), methods=np.zeros(max(nb, 1), np.uint8),
+        arr = dict(data=a, methods=np.zeros(max(nb, 1), np.uint8),
                    lens=np.zeros(max(nb, 1), np.uint32), offs=np.zeros(max(nb, 1), np.uint64),
                    crcs=np.zeros(max(nb, 1), np.uint32))
+        arr["payloads"] = self._buf(max(a.size, 1), arr, "payloads")
         j = _Job(JOB_COMPRESS, block_log, level, _ptr(a), a.size, 0, None, None, None, None, _ptr(arr["payloads"]),
                  arr["payloads"].size, _ptr(arr["methods"]), _ptr(arr["lens"]), _ptr(arr["offs"]), _ptr(arr["crcs"]))
         h = ServeJob(JOB_COMPRESS, arr)
         h.nb = nb
-        return self._submit(j, h)
+        return self._submit(j, self._track(h))
 
     def _decode(self, kind, comp, comp_lens, methods, raw_lens, block_log, crcs_expected=None):
         c = _as_u8(comp)
@@ -421,13 +445,13 @@ class Server:
         arr = dict(comp=c, comp_lens=cl, methods=me, raw_lens=rl, crcs=np.zeros(max(nb, 1), np.uint32))
         out = None
         if kind == JOB_EXTRACT:
-            out = arr["raw"] = np.empty(max(int(rl.sum()), 1), np.uint8)
+            out = arr["raw"] = self._buf(max(int(rl.sum()), 1), arr, "raw")
         exp = None
         if crcs_expected is not None:
             exp = arr["crcs_expected"] = np.ascontiguousarray(crcs_expected, np.uint32)
         j = _Job(kind, block_log, 0, _ptr(c), c.size, nb, _ptr(cl), _ptr(me), _ptr(rl), _ptr(exp), _ptr(out),
                  0 if out is None else out.size, None, None, None, _ptr(arr["crcs"]))
-        return self._submit(j, ServeJob(kind, arr))
+        return self._submit(j, self._track(ServeJob(kind, arr)))
 
     def extract(self, comp, comp_lens, methods, raw_lens, block_log=18):
         """Record bodies back to back -> raw bytes (handle.raw) and CRCs (handle.crcs)."""
@@ -448,7 +472,10 @@ class Server:
     def stats(self):
         v = [C.c_uint64() for _ in range(4)]
         lib().zc_serve_stats(self._srv, *[C.byref(x) for x in v])
-        return dict(jobs_done=v[0].value, raw_bytes=v[1].value, ticks=v[2].value, arena_used=v[3].value)
+        t = [C.c_double() for _ in range(4)]
+        lib().zc_serve_times(self._srv, *[C.byref(x) for x in t])
+        return dict(jobs_done=v[0].value, raw_bytes=v[1].value, ticks=v[2].value, arena_used=v[3].value,
+                    gpu_s=t[0].value, wait_s=t[1].value, handout_s=t[2].value, upload_s=t[3].value)
 
 
 def record_bodies(data, methods, lens, payloads, offs, block_log):
