@@ -440,7 +440,20 @@ __device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x) {
     if (live != chain || chain != kFull) stop = true;  // the chain ends in this chunk
     const bool on = (live >> lane) & 1u;
     const uint32_t j = on ? P.spos[r - k] : 0u;
-    const uint32_t l = on ? lcp(P.in, P.base + j, ax, l32) : 0u;
+    uint32_t l = 0;
+    if (on) {  // 16 bytes a round from independent word loads (at most two rounds)
+      const uint64_t aj = P.base + j;
+      for (uint32_t o = 0; o < l32; o += 16) {
+        uint32_t x[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) x[q] = load4(P.in, aj + o + 4 * q) ^ load4(P.in, ax + o + 4 * q);
+        uint32_t k = 16;
+#pragma unroll
+        for (int q = 3; q >= 0; --q) if (x[q]) k = 4 * q + (((uint32_t)__ffs(x[q]) - 1u) >> 3);
+        l = min(o + k, l32);
+        if (k < 16) break;
+      }
+    }
     // candidates shorter than 32 bytes (or the whole remaining length): the longest, nearest on a tie
     uint32_t key = on ? (l << 8) | (31u - lane) : 0u;  // (l <= 32, lanes in chain order)
     key = __reduce_max_sync(kFull, key);
