@@ -131,18 +131,34 @@ __global__ void __launch_bounds__(64) k_dec_streams(DecArgs A) {
   }
   __syncthreads();
   if (fail) { if (k == 0) set_err(A.err, b, E_LANE); return; }
-  // 64 lanes: lane k decodes symbols k, k+64, ...
+  // 64 lanes: lane k decodes symbols k, k+64, ...  The lane's bytes come through a register buffer filled
+  // from aligned words, the next word loaded at least two symbols before it is needed (a symbol takes at
+  // most two bytes); the words may extend up to 8 bytes past the lane, inside the input's readable slack.
   const uint8_t* in = body + hdr + lstart[k];
-  const uint8_t* in_end = in + ll;
   uint32_t x = ld32(in);
   in += 4;
+  uint32_t rem = ll - 4;  // the lane's bytes not yet taken
+  const uint32_t* wp = reinterpret_cast<const uint32_t*>((uintptr_t)in & ~(uintptr_t)3);
+  const uint32_t skip = (uint32_t)((uintptr_t)in & 3u);
+  uint64_t buf = __ldg(wp) >> (8 * skip);
+  uint32_t nbuf = 4 - skip;
+  uint32_t nxt = __ldg(wp + 1);
+  wp += 1;
   for (uint32_t i = k; i < ns; i += kLanes) {
+    if (nbuf < 4) {
+      buf |= (uint64_t)nxt << (8 * nbuf);
+      nbuf += 4;
+      nxt = __ldg(++wp);
+    }
     const uint32_t e = tab[x & (kScale - 1)];
     dest[i] = (uint8_t)e;
     x = (((e >> 8) & 0xFFFu) + 1u) * (x >> kScaleBits) + (e >> 20);
     while (x < kRansLow) {
-      if (in >= in_end) { set_err(A.err, b, E_LANE); return; }
-      x = (x << 8) | *in++;
+      if (rem == 0) { set_err(A.err, b, E_LANE); return; }
+      x = (x << 8) | (uint32_t)(buf & 0xFFu);
+      buf >>= 8;
+      --nbuf;
+      --rem;
     }
   }
 }
