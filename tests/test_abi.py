@@ -61,3 +61,10 @@ def test_host_crc_combine_matches_oracle(so):
         a, b, n = rng.getrandbits(32), rng.getrandbits(32), rng.randrange(0, 1 << 36)
         assert Z.crc32_combine(a, b, n) == O.Port.crc32_combine(a, b, n)
 
+
+
+def test_library_resolves_every_symbol_at_load(so):
+    """Loaded with immediate binding, and no symbol of the codec's own namespace left undefined."""
+    ctypes.CDLL(so, mode=os.RTLD_NOW)
+    out = subprocess.run(["nm", "-D", "--undefined-only", so], capture_output=True, text=True).stdout
+    assert not re.findall(r"\b_ZN2zc\w+", out)
