@@ -500,9 +500,11 @@ __device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x) {
 
 // One step of the CPU parse (src/codec2.h:69-80) for every lane with `act` (all 32 lanes call it):
 // returns the next position (p itself when !act); the token, when the step emits one, in (ti, tm, td).
-// Capped records at p or p + 1 are finished first, one at a time, by the whole warp.
-__device__ __forceinline__ uint32_t warp_step(const ParseBlock& P, uint32_t p, bool act, bool& tok, uint32_t& ti,
-                                              uint32_t& tm, uint32_t& td) {
+// Capped records at p or p + 1 are finished first, one at a time, by the whole warp.  A position with
+// no match is a literal step to the next position, so a run of them is taken at once, up to `lim` (the
+// walk's end): the walk lands where the CPU parse's single steps would first leave the run or reach lim.
+__device__ __forceinline__ uint32_t warp_step(const ParseBlock& P, uint32_t p, uint32_t lim, bool act, bool& tok,
+                                              uint32_t& ti, uint32_t& tm, uint32_t& td) {
   uint32_t v = act ? P.minfo[p] : M_NONE;
   const bool lz = act && v != M_NONE && p + 1 < P.n;
   uint32_t v2 = lz ? P.minfo[p + 1] : M_NONE;
@@ -522,7 +524,20 @@ __device__ __forceinline__ uint32_t warp_step(const ParseBlock& P, uint32_t p, b
   }
   tok = false;
   if (!act) return p;
-  if (v == M_NONE) return p + 1;
+  if (v == M_NONE) {
+    const uint32_t* m = P.minfo;
+    uint32_t q = p + 1;
+    while (q + 4 <= lim) {
+      const uint32_t a0 = m[q], a1 = m[q + 1], a2 = m[q + 2], a3 = m[q + 3];
+      if (a0 != M_NONE) break;
+      if (a1 != M_NONE) { q += 1; break; }
+      if (a2 != M_NONE) { q += 2; break; }
+      if (a3 != M_NONE) { q += 3; break; }
+      q += 4;
+    }
+    while (q < lim && m[q] == M_NONE) ++q;
+    return q;
+  }
   uint32_t m = m_len(v), d = m_dist(v), at = p;
   if (lz && v2 != M_NONE) {
     const uint32_t m2 = m_len(v2), d2 = m_dist(v2);
@@ -551,7 +566,7 @@ __global__ void __launch_bounds__(256, 8) k_enc_parse(EncArgs A) {  // (8 CTAs a
   // round 0: every segment walked from its own start
   {
     uint32_t p = s;
-    while (__any_sync(kFull, p < e)) p = warp_step(P, p, p < e, t, ta, tc, td);
+    while (__any_sync(kFull, p < e)) p = warp_step(P, p, e, p < e, t, ta, tc, td);
     ent[q] = s;
     ex[q] = s < e ? p : s;
   }
@@ -572,7 +587,7 @@ __global__ void __launch_bounds__(256, 8) k_enc_parse(EncArgs A) {  // (8 CTAs a
     }
     while (__any_sync(kFull, mode != 0)) {
       const bool adv_a = mode == 1 || (mode == 2 && a < c);
-      const uint32_t y = warp_step(P, adv_a ? a : c, mode != 0, t, ta, tc, td);
+      const uint32_t y = warp_step(P, adv_a ? a : c, e, mode != 0, t, ta, tc, td);
       if (mode == 1) {
         a = y;
         if (a >= e) { nx = a; mode = 0; }
@@ -597,7 +612,7 @@ __global__ void __launch_bounds__(256, 8) k_enc_parse(EncArgs A) {  // (8 CTAs a
   uint32_t* gd = gm + seg_tok_cap(A.B);
   uint32_t cnt = 0;
   for (uint32_t p = from; __any_sync(kFull, p < e);) {
-    p = warp_step(P, p, p < e, t, ta, tc, td);
+    p = warp_step(P, p, e, p < e, t, ta, tc, td);
     if (t) { gi[cnt] = ta; gm[cnt] = tc; gd[cnt] = td; ++cnt; }
   }
   const uint32_t incl = warp_incl_scan(cnt);
