@@ -304,3 +304,35 @@ def test_host_calls_in_chunks_match_one_device_call(codec):
     raw, dcrcs, errs = codec.decompress_arrays(blob, coffs, [x.size for x in comp], meth,
                                                [min(B, n - b * B) for b in range(nb)])
     assert not errs.any() and np.array_equal(raw[:n], data) and np.array_equal(dcrcs, crcs)
+
+
+@pytest.mark.parametrize("block_log,level", [(20, 1), (20, 9), (16, 5)])
+def test_adversarial_multi_block_parity(codec, block_log, level):
+    """Long zero runs, short periods, far copies and single-byte runs across several blocks: chains of equal
+    hashes at full depth, 4096-byte matches, overlapping copies.  Payloads byte-identical to the oracle."""
+    import datagen as G
+    rng = np.random.default_rng(5150 + block_log + level)
+    far = rng.integers(0, 256, 100000, dtype=np.uint8)
+    runs = np.concatenate([np.full(int(k), int(v), np.uint8) for k, v in
+                           zip(rng.integers(1, 300, 2000), rng.integers(0, 4, 2000))])
+    parts = [np.zeros(300000, np.uint8), np.frombuffer(b"abc" * 70000, np.uint8), far,
+             rng.integers(0, 256, 50000, dtype=np.uint8), far, runs, G.lz_mix(200000, block_log, 77),
+             np.frombuffer(b"\x00\x01" * 40000, np.uint8)]
+    data = np.concatenate(parts).tobytes()
+    B = 1 << block_log
+    methods, lens, crcs, pay, offs = codec.compress_arrays(data, block_log, level=level)
+    want = cpu_blocks(data, block_log, level)
+    comp = []
+    for b, (m, p) in enumerate(want):
+        blk = data[b * B:(b + 1) * B]
+        assert methods[b] == m, b
+        if m:
+            got = pay[int(offs[b]): int(offs[b]) + int(lens[b])].tobytes()
+            assert got == p, b
+            comp.append(got)
+        else:
+            comp.append(blk)
+    coffs = np.cumsum([0] + [len(c) for c in comp[:-1]])
+    raw_lens = [min(B, len(data) - b * B) for b in range(len(want))]
+    raw, dcrcs, errs = codec.decompress_arrays(b"".join(comp), coffs, [len(c) for c in comp], methods, raw_lens)
+    assert not errs.any() and raw.tobytes() == data and list(dcrcs) == list(crcs)
