@@ -137,6 +137,7 @@ struct zc_ctx {
   // staging for the host-pointer calls
   DevBuf s_in, s_blk, s_out, s_meta;
   HostBuf h_meta;
+  DevBuf work;  // the decoder fill's device work counter
   // the host-pointer codec calls run in chunks through two stages: a chunk's copies (on cstream) overlap
   // the other chunk's kernels (on stream)
   struct Stage {
@@ -302,6 +303,7 @@ int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs,
   A.tk_lik = c->d_tkl.as<uint32_t>(); A.tot_op = c->d_tot.as<uint32_t>(); A.tot_li = A.tot_op + nb;
   const Shape& sh = c->shape[block_log - zc::kMinBlockLog][level_class(c->level)];
   A.ring_log = sh.ring_log; A.fill_warps = sh.fill_warps;
+  A.work = c->work.as<uint32_t>() + 1;
   zc::launch_decode_fill(A, st, c->stages);
   if (d_crcs && nb) {
     zc::CrcArgs C{};
@@ -485,6 +487,7 @@ int zc_open(zc_ctx** out, int device) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&S.ev_done, cudaEventDisableTiming);
   }
   if (e == cudaSuccess) e = zc::prepare_kernels();
+  if (e == cudaSuccess) e = grow(c->work, 256);
   if (e == cudaSuccess) e = cudaMalloc(&c->d_crct, sizeof(zc::CrcTables));
   if (e == cudaSuccess) {
     zc::CrcTables T;
@@ -508,7 +511,7 @@ void zc_close(zc_ctx* c) {
   for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_minfo, &c->e_scnt, &c->e_tk_seg, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
                     &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
                     &c->e_bits, &c->e_lanes, &c->e_freq, &c->e_lanelen, &c->e_sinfo, &c->e_slab, &c->d_lit, &c->d_tok,
-                    &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta})
+                    &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta, &c->work})
     release(*b);
   if (c->h_meta.p) cudaFreeHost(c->h_meta.p);
   for (auto& S : c->pipe) {

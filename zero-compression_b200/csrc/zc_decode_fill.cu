@@ -10,6 +10,8 @@
 //                 lanes (a group's matches read only output from before the group, or their own
 //                 literals), the next 32 tokens' table loaded while the current ones are filled.
 // Stored blocks are copied by k_dec_fill.  The rANS streams come from k_dec_streams (zc_decode.cu).
+#include <algorithm>
+
 #include "zc_internal.cuh"
 #include "zc_kernels.h"
 
@@ -305,16 +307,9 @@ __device__ inline void copy_bytes(uint8_t* d, const uint8_t* s, uint32_t n) {  /
 
 }  // namespace
 
-// One warp per block; a CTA holds blockDim.x / 32 warps, each with its table and a ring of 2^ring_log
-// bytes in dynamic shared memory (16-byte aligned, the ring after the table).
-__global__ void __launch_bounds__(256) k_dec_fill(DecArgs A) {
-  extern __shared__ __align__(16) uint8_t fsm[];
+// The replay of block b by one warp, with the warp's table and ring.
+__device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTable& T, uint8_t* ring) {
   const uint32_t R = 1u << A.ring_log;
-  const uint32_t wid = threadIdx.x >> 5;
-  const uint32_t b = blockIdx.x * (blockDim.x >> 5) + wid;
-  if (b >= A.nb) return;
-  FillTable& T = *reinterpret_cast<FillTable*>(fsm + (size_t)wid * (kTableBytes + R));
-  uint8_t* ring = fsm + (size_t)wid * (kTableBytes + R) + kTableBytes;
   const uint32_t lane = lane_id();
   const uint32_t raw = A.raw_len[b], method = A.method[b], clen = A.comp_len[b], B = A.B;
   uint8_t* o = A.out + A.out_off[b];
@@ -386,6 +381,26 @@ __global__ void __launch_bounds__(256) k_dec_fill(DecArgs A) {
   copy_bytes(o + op_total, lit + li_total, m.nl - li_total);
 }
 
+// Fed by a device work queue: every warp takes the next block from the work counter until none is left,
+// so blocks of uneven sizes (a batch of many files) balance across warps.  A CTA holds blockDim.x / 32 warps, each
+// with its table and a ring of 2^ring_log bytes in dynamic shared memory (16-byte aligned, the ring after
+// the table).  The ring is read only at positions the warp has written in its current block.
+__global__ void __maxnreg__(72) k_dec_fill(DecArgs A) {  // (72 registers: 28 warps an SM with 4-warp CTAs)
+  extern __shared__ __align__(16) uint8_t fsm[];
+  const uint32_t R = 1u << A.ring_log;
+  const uint32_t wid = threadIdx.x >> 5;
+  FillTable& T = *reinterpret_cast<FillTable*>(fsm + (size_t)wid * (kTableBytes + R));
+  uint8_t* ring = fsm + (size_t)wid * (kTableBytes + R) + kTableBytes;
+  for (;;) {
+    uint32_t b = 0;
+    if (lane_id() == 0) b = atomicAdd(A.work, 1u);
+    b = __shfl_sync(kFull, b, 0);
+    if (b >= A.nb) break;
+    fill_block(A, b, T, ring);
+    __syncwarp();
+  }
+}
+
 size_t fill_smem_bytes(uint32_t ring_log, uint32_t warps) { return (size_t)warps * (kTableBytes + (1u << ring_log)); }
 
 cudaError_t prepare_fill() {
@@ -403,8 +418,10 @@ void launch_decode_fill(const DecArgs& A, cudaStream_t st, Stages& S) {
   S.end(st);
   const uint32_t W = A.fill_warps;
   const size_t sm = fill_smem_bytes(A.ring_log, W);
+  const uint32_t grid = (A.nb + W - 1) / W;  // (as many warps as blocks; the counter balances them)
+  cudaMemsetAsync(A.work, 0, sizeof(uint32_t), st);
   S.begin("k_dec_fill", st);
-  k_dec_fill<<<(A.nb + W - 1) / W, 32 * W, sm, st>>>(A);
+  k_dec_fill<<<grid, 32 * W, sm, st>>>(A);
   S.end(st);
 }
 

@@ -42,6 +42,7 @@ struct DecArgs {
   uint32_t *tot_op, *tot_li;
   // the fill's shape: a ring of 2^ring_log recent output bytes per warp, fill_warps warps (blocks) per CTA
   uint32_t ring_log, fill_warps;
+  uint32_t* work;             // the fill's device work counter (zeroed by the launcher)
 };
 
 constexpr uint32_t kMinFillRingLog = 11, kMaxFillRingLog = 15, kMaxFillWarps = 8;
