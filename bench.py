@@ -530,6 +530,167 @@ def run_batched(args):
     return 0 if plain["bit_exact"] and batched["bit_exact"] else 1
 
 
+def run_archive(args):
+    """Whole-archive workload: the many-file set of the batched config written as one .zero archive whose
+    records, file CRCs (over each file's span, across blocks), entry table and footer are assembled on
+    the GPU, then extracted with every block and file CRC checked.  value: the device-resident write
+    (zc_archive_write_device), raw GB / CUDA-event time.  e2e: write + extract through the host-pointer
+    calls (zc_archive_write, zc_archive_extract) with pinned buffers, copies included.  The reference's
+    compress_archive (CPU codec, all host threads) writes a sample of the same files from the page cache,
+    and the GPU writer's bytes for that sample must equal its archive."""
+    import ctypes as C
+    import shutil
+    import tempfile
+    import numpy as np
+    import torch
+    import zero_cuda as Z
+    import datagen as G
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    bl, level = args.block, args.level
+    sizes, kinds = G.file_plan(args.files, 1 << 10, args.max_file_kib << 10, seed=2024)
+    sizes = sizes.astype(np.int64)
+    file_off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    total = int(sizes.sum())
+    pinned = torch.zeros(total + 64, dtype=torch.uint8, pin_memory=True)
+    hv = pinned.numpy()
+    for f in range(args.files):
+        o = int(file_off[f])
+        hv[o:o + int(sizes[f])] = G.by_kind(int(kinds[f]), int(sizes[f]), bl, 5000 + f)
+    ext = ("txt", "lz", "rnd")
+    entries = []
+    for f in range(args.files):
+        if f % 250 == 0:
+            entries.append(Z.ArchiveEntry("d%03d" % (f // 250), 0, mtime=1700000000, is_dir=True))
+        entries.append(Z.ArchiveEntry("d%03d/f%05d.%s" % (f // 250, f, ext[int(kinds[f])]), int(sizes[f]),
+                                      mtime=1700000000 + f))
+    ne = len(entries)
+    L = Z.lib()
+    arr, _keep = Z._c_entries(entries)
+    cap = Z.archive_bound(entries, bl)
+    codec = Z.CudaCodec(level=level, device=local)
+    d_solid = torch.zeros(total + 64, dtype=torch.uint8, device=dev)
+    d_solid.copy_(pinned)
+    d_out = torch.zeros(cap, dtype=torch.uint8, device=dev)
+    d_len = torch.zeros(1, dtype=torch.int64, device=dev)
+    d_ecrc = torch.zeros(ne, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+
+    def check(rc):
+        if rc:
+            Z._raise(codec._ctx, rc)
+
+    def write_dev():
+        check(L.zc_archive_write_device(codec._ctx, d_solid.data_ptr(), bl, level, arr, ne, d_out.data_ptr(), cap,
+                                        d_len.data_ptr(), d_ecrc.data_ptr(), sh))
+
+    for _ in range(args.warmup):
+        write_dev()
+    torch.cuda.synchronize(dev)
+    ev = _events(args.steps)
+    l0 = codec.launch_count()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                ev[i][0].record(stream)
+                write_dev()
+                ev[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+    t_w = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+    launches = (codec.launch_count() - l0) // args.steps
+    alen = int(d_len.item())
+    dev_arch = d_out[:alen].cpu().numpy()
+    codec.profile(True)
+    write_dev()
+    torch.cuda.synchronize(dev)
+    stages = codec.profile_stages()
+    codec.profile(False)
+    # e2e: the host-pointer write and extract, pinned buffers
+    h_arch = torch.zeros(cap, dtype=torch.uint8, pin_memory=True).numpy()
+    h_back = torch.zeros(total + 64, dtype=torch.uint8, pin_memory=True).numpy()
+    out_len = C.c_uint64()
+
+    def e2e_step():
+        check(L.zc_archive_write(codec._ctx, hv.ctypes.data, bl, level, arr, ne, h_arch.ctypes.data, cap,
+                                 C.byref(out_len)))
+        check(L.zc_archive_extract(codec._ctx, h_arch.ctypes.data, out_len.value, h_back.ctypes.data, total))
+
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    t_e = (time.perf_counter() - t0) / args.steps
+    ok = (out_len.value == alen and np.array_equal(h_arch[:alen], dev_arch)
+          and np.array_equal(h_back[:total], hv[:total])
+          and [int(x) & 0xFFFFFFFF for x in d_ecrc.cpu().tolist()] == [int(arr[i].crc) for i in range(ne)])
+    info, _ = Z.read_table(dev_arch)
+    line = {"metric": METRIC, "value": round(total / t_w / 1e6, 3), "unit": "GB/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_w, 3), "higher_is_better": True,
+            "scaling": "weak", "dtype": "u8", "data": "synthetic (seeded per-file generators)",
+            "config": {"workload": f"archive: {args.files} files in {ne - args.files} folders, sizes log-uniform "
+                                   f"1 KiB-{args.max_file_kib} KiB ({total / 2**30:.2f} GiB), generators "
+                                   f"text/lz/random, block {bl}, level {level}: the whole .zero archive written on "
+                                   f"the GPU (records, file CRCs, table, footer)",
+                       "blocks": int(info["n_blocks"]), "bytes": total, "archive_bytes": alen,
+                       "l2_flush": "none needed: input larger than the 126 MB L2"},
+            "ratio": round(alen / total, 5), "bit_exact": bool(ok), "gpu_launches": launches,
+            "stages_ms_per_step": {k: round(v[0], 4) for k, v in stages.items()},
+            "e2e": {"value": round(total / t_e / 1e9, 4), "unit": "GB/s",
+                    "h2d_bytes_per_step": int(total + alen), "d2h_bytes_per_step": int(alen + total),
+                    "path": "zc_archive_write + zc_archive_extract (every block and file CRC checked), pinned "
+                            "host buffers"},
+            "clocks": clk.summary()}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        if O.Ref.available():
+            base = "/dev/shm" if os.path.isdir("/dev/shm") else None
+            tmp = tempfile.mkdtemp(prefix="zc_arch_", dir=base)
+            try:
+                root = os.path.join(tmp, "data")
+                picked = 0
+                for e in entries:
+                    p = os.path.join(root, e.name)
+                    if e.is_dir:
+                        os.makedirs(p, exist_ok=True)
+                        continue
+                    if picked >= (256 << 20):
+                        break
+                    f = int(e.name.split("/f")[1].split(".")[0])
+                    with open(p, "wb") as fh:
+                        fh.write(hv[int(file_off[f]):int(file_off[f]) + e.size].tobytes())
+                    picked += e.size
+                for dp, dn, fn in os.walk(root):
+                    for x in dn + fn:
+                        os.utime(os.path.join(dp, x), (1700000000, 1700000000))
+                os.utime(root, (1700000000, 1700000000))
+                zpath = os.path.join(tmp, "ref.zero")
+                t0 = time.perf_counter()
+                O.Ref.compress_archive([root], zpath, block_log=bl, level=level)
+                t_ref = time.perf_counter() - t0
+                with open(zpath, "rb") as fh:
+                    ref = fh.read()
+                _, rents = Z.read_table(ref)
+                solid = b"".join(open(os.path.join(tmp, e.name), "rb").read() for e in rents if not e.is_dir)
+                same = codec.archive_write(solid, rents, bl, level=level) == ref
+                line["cpu_baseline"] = {"value": round(picked / t_ref / 1e9, 4), "unit": "GB/s",
+                                        "cores": O.Ref.hardware_threads(), "kind": "reference",
+                                        "sample": f"compress_archive of the first {picked >> 20} MiB of the files "
+                                                  f"(page cache), CPU codec, block {1 << bl >> 10} KiB, level {level}"}
+                line["same_as_reference_archive"] = bool(same)
+                ok = ok and same
+            finally:
+                shutil.rmtree(tmp, ignore_errors=True)
+    line["bit_exact"] = bool(ok)
+    print(json.dumps(line), flush=True)
+    codec.close()
+    return 0 if ok else 1
+
+
 def run_decode(args):
     """Decode-heavy workload (the decode config, scaled): LZ-mix data at block 2^20, level 9, compressed
     once (untimed; the GPU encoder writes the reference CPU codec's bytes), then extracted K times.  Each
@@ -755,8 +916,9 @@ def main():
     ap.add_argument("--level", type=int, default=None, help="default 5; 9 for --config decode")
     ap.add_argument("--size-mib", type=int, default=None, help="default 1024; 8192 for --config decode")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--config", choices=["lz", "batched", "decode", "serve"], default="lz",
-                    help="lz: the headline round trip; batched: many files, plain vs batched; decode: extract-heavy")
+    ap.add_argument("--config", choices=["lz", "batched", "decode", "serve", "archive"], default="lz",
+                    help="lz: the headline round trip; batched: many files, plain vs batched; decode: extract-heavy; "
+                         "serve: the request loop; archive: whole .zero archives of many files")
     ap.add_argument("--files", type=int, default=10000)
     ap.add_argument("--max-file-kib", type=int, default=1024)
     ap.add_argument("--pool", type=int, default=48, help="serve: distinct files the jobs draw from")
@@ -780,6 +942,8 @@ def main():
         return run_decode(args)
     if args.config == "serve":
         return run_serve(args)
+    if args.config == "archive":
+        return run_archive(args)
     return run_ours(args)
 
 

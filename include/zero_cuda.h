@@ -221,6 +221,79 @@ int zc_serve_stats(zc_server *srv, uint64_t *jobs_done, uint64_t *raw_bytes, uin
 int zc_crc32(zc_ctx *ctx, const uint8_t *data, size_t n, uint32_t *crc);
 uint32_t zc_crc32_combine(uint32_t crc_a, uint32_t crc_b, uint64_t len_b);
 
+/* ---- whole archives: the .zero container around the blocks, assembled on the GPU.
+ * Layout (src/archive.h:334-441 writes it, 451-495 reads its table):
+ *   header   "ZERO", u8 version 2, u8 block_log, u16 0, u64 total raw bytes, u64 blocks
+ *   records  per block: u32 raw_len, u32 comp_len, u8 method, 3 zero bytes, u32 CRC-32 of the raw block,
+ *            then comp_len bytes (the ZB2 payload, or the raw bytes when stored)
+ *   table    u32 entries; per entry u8 type (1 = folder), 3 zero bytes, u32 name length, the name,
+ *            u64 size, u64 mtime, u32 attributes, u32 CRC-32 of the file's bytes
+ *   footer   u64 table offset, u64 table length, u32 CRC-32 of the table, "ZEND"
+ * The files' bytes follow one another in entry order as one solid stream cut into blocks of
+ * 2^block_log (only the last block is shorter), so a file may straddle blocks. */
+typedef struct {
+  const char *name;   /* the entry's '/'-separated relative name: name_len bytes, not NUL-terminated */
+  uint32_t name_len;
+  uint32_t is_dir;    /* 1: a folder (no bytes in the stream; its size must be 0) */
+  uint64_t size;      /* the file's bytes in the solid stream */
+  int64_t mtime;
+  uint32_t attr;
+  uint32_t crc;       /* CRC-32 of the file's bytes (0 for folders and empty files) */
+} zc_entry;
+
+typedef struct {
+  uint32_t block_log;
+  uint32_t n_entries;
+  uint64_t total_raw;   /* bytes of the solid stream (the sum of the files' sizes) */
+  uint64_t n_blocks;
+  uint64_t table_off;   /* where the entry table starts: the records lie in [24, table_off) */
+  uint64_t table_len;
+} zc_archive_info;
+
+/* The largest archive that zc_archive_write can produce for these entries (every block stored). */
+uint64_t zc_archive_bound(const zc_entry *entries, uint32_t n_entries, uint32_t block_log);
+
+/* Writes a whole archive of the solid stream d_solid (the files' bytes in entry order, sum of the sizes
+ * bytes; 16-byte aligned with 64 readable bytes after the end, as zc_compress_device's input) into
+ * d_out (out_cap >= zc_archive_bound bytes), all on the GPU: the records are placed by a device scan,
+ * the files' CRCs (crc32 over each file's span, across block boundaries) are computed on the device and
+ * written into the table, whose CRC and the footer follow.  *d_len (device u64) gets the archive's
+ * length; d_entry_crcs (device, n_entries; may be NULL) each entry's CRC.  Work is queued on `stream`;
+ * the call returns once it is queued.  At the same level, the bytes equal those compress_archive
+ * (src/archive.h:334-441) writes with the reference CPU codec for the same entries. */
+int zc_archive_write_device(zc_ctx *ctx, const uint8_t *d_solid, uint32_t block_log, int level,
+                            const zc_entry *entries, uint32_t n_entries, uint8_t *d_out, uint64_t out_cap,
+                            uint64_t *d_len, uint32_t *d_entry_crcs, void *stream);
+
+/* The same from host memory into host memory (synchronous): solid holds the files' bytes in entry order;
+ * *out_len gets the archive's length and entries[i].crc each entry's CRC. */
+int zc_archive_write(zc_ctx *ctx, const uint8_t *solid, uint32_t block_log, int level, zc_entry *entries,
+                     uint32_t n_entries, uint8_t *out, uint64_t out_cap, uint64_t *out_len);
+
+/* Reads the header, footer and entry table of an archive held in host memory, arch[0 .. len), with the
+ * checks of read_info (src/archive.h:451-495): the magic, version 2, the block size, the footer, the
+ * table's position and CRC, every entry inside the table, and the files' sizes summing to the header's
+ * total.  info gets the layout; entries (may be NULL) the first `cap` entries, their names pointing into
+ * arch.  Host-only: needs no GPU and no context.  ZC_E_DATA on a damaged archive, the reason in msg
+ * (msg_cap bytes, NUL-terminated; may be NULL). */
+int zc_archive_read_table(const uint8_t *arch, uint64_t len, zc_archive_info *info, zc_entry *entries,
+                          uint32_t cap, char *msg, size_t msg_cap);
+
+/* Walks the block records of an archive in host memory (src/archive.h:566-586) with the same checks:
+ * a raw length within the block size, a stored block's lengths equal, a known method, no body past the
+ * table.  Per block b: offs[b] where its body starts in arch, comp_lens, methods, raw_lens and the
+ * record's CRC in crcs (each array info->n_blocks long; crcs may be NULL).  Host-only, as above. */
+int zc_archive_blocks(const uint8_t *arch, uint64_t len, const zc_archive_info *info, uint64_t *offs,
+                      uint32_t *comp_lens, uint8_t *methods, uint32_t *raw_lens, uint32_t *crcs, char *msg,
+                      size_t msg_cap);
+
+/* Extracts (out != NULL: the solid stream, info.total_raw bytes, into out) or only tests (out == NULL) an
+ * archive held in host memory, as read_blocks + extract_archive / test_archive do (src/archive.h:566-635,
+ * 747-785): every block decoded on the GPU, each block's CRC checked against its record, each file's
+ * CRC (over its span of the solid stream) computed on the GPU and checked against the table.  ZC_E_DATA
+ * for the first failing check, its message in zc_last_error. */
+int zc_archive_extract(zc_ctx *ctx, const uint8_t *arch, uint64_t len, uint8_t *out, uint64_t out_cap);
+
 /* Kernel launches this context has issued since it was opened (for accounting). */
 uint64_t zc_launch_count(const zc_ctx *ctx);
 

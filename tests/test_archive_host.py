@@ -1,0 +1,198 @@
+"""The archive container's host side, on the CPU: the table and record readers of libzero_cuda.so
+(zc_archive_read_table, zc_archive_blocks -- host-only, no GPU) against archives the reference's own
+compress_archive wrote (the golden fixtures), and against the reference reader's error for every kind of
+damage it detects in the header, footer, table and block records (src/archive.h:451-495, 566-586).
+The blocks themselves are decoded here by the oracle."""
+import os
+import struct
+import zlib
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_manifest
+
+import oracle as O
+import zero_cuda as Z
+
+ARCH_DIR = os.path.join(GOLDEN, "archives", "three_files")
+
+
+def golden(name):
+    with open(os.path.join(ARCH_DIR, name + ".zero"), "rb") as f:
+        return f.read()
+
+
+def solid_of(entries, root):
+    """The files' bytes in entry order (the solid stream), read from the fixture's source tree."""
+    out = bytearray()
+    for e in entries:
+        if not e.is_dir:
+            with open(os.path.join(root, e.name), "rb") as f:
+                out += f.read()
+    return bytes(out)
+
+
+def test_golden_tables_match_the_files():
+    for ent in load_manifest()["archives"]:
+        a = golden(ent["name"])
+        info, es = Z.read_table(a)
+        assert info["block_log"] == ent["block_log"] == 16
+        solid = solid_of(es, ARCH_DIR)
+        assert info["total_raw"] == len(solid)
+        assert info["n_blocks"] == (len(solid) + (1 << 16) - 1) >> 16
+        assert info["table_off"] + info["table_len"] + 24 == len(a)
+        for e in es:
+            if e.is_dir:
+                assert e.size == 0 and e.crc == 0 and os.path.isdir(os.path.join(ARCH_DIR, e.name))
+            else:
+                with open(os.path.join(ARCH_DIR, e.name), "rb") as f:
+                    data = f.read()
+                assert e.size == len(data) and e.crc == zlib.crc32(data)
+
+
+def test_golden_records_decode_with_the_oracle():
+    for ent in load_manifest()["archives"]:
+        a = golden(ent["name"])
+        info, es = Z.read_table(a)
+        rec = Z.archive_blocks(a, info)
+        solid = solid_of(es, ARCH_DIR)
+        B = 1 << info["block_log"]
+        out = bytearray()
+        for b in range(info["n_blocks"]):
+            o, cl, m, rl = int(rec["offs"][b]), int(rec["comp_lens"][b]), int(rec["methods"][b]), int(rec["raw_lens"][b])
+            body = a[o:o + cl]
+            raw = body if m == 0 else O.Port.decompress_block(body, rl)
+            assert rl == min(B, len(solid) - b * B)
+            assert int(rec["crcs"][b]) == zlib.crc32(raw)
+            out += raw
+        assert bytes(out) == solid
+
+
+def test_bound_counts_every_part():
+    es = [Z.ArchiveEntry("d", 0, is_dir=True), Z.ArchiveEntry("d/f", 100000), Z.ArchiveEntry("e", 0)]
+    table = 4 + sum(8 + len(e.name) + 24 for e in es)
+    assert Z.archive_bound(es, 16) == 24 + 2 * 16 + 100000 + table + 24
+    assert Z.archive_bound(es, 15) == 0                              # block size out of range
+    assert Z.archive_bound([Z.ArchiveEntry("d", 5, is_dir=True)], 16) == 0  # a folder with bytes
+
+
+# ---- damage: each mutation of a golden archive, our reader's message and the reference reader's
+
+def fix_table_crc(a):
+    """Recomputes the footer's table CRC after an edit inside the table."""
+    b = bytearray(a)
+    toff, tl = struct.unpack_from("<QQ", b, len(b) - 24)
+    struct.pack_into("<I", b, len(b) - 8, zlib.crc32(bytes(b[toff:toff + tl])))
+    return bytes(b)
+
+
+def mutate(a, what):
+    b = bytearray(a)
+    toff, tl = struct.unpack_from("<QQ", b, len(b) - 24)
+    if what == "magic":
+        b[0] = ord("X")
+    elif what == "version":
+        b[4] = 3
+    elif what == "block_size":
+        b[5] = 15
+    elif what == "too_short":
+        b = b[:40]
+    elif what == "footer":
+        b = b[:-1]
+    elif what == "table_position":
+        struct.pack_into("<Q", b, len(b) - 24, toff + 1)
+    elif what == "table_checksum":
+        b[toff + 6] ^= 1
+    elif what == "entry_cut":
+        struct.pack_into("<I", b, toff, 7)  # more entries than the table holds
+        return fix_table_crc(b)
+    elif what == "entry_name":
+        struct.pack_into("<I", b, toff + 4 + 4, 10 ** 6)  # the first name runs past the table
+        return fix_table_crc(b)
+    elif what == "sizes":
+        struct.pack_into("<Q", b, 8, struct.unpack_from("<Q", b, 8)[0] + 1)
+    elif what == "rec_raw_len":
+        struct.pack_into("<I", b, 24, (1 << 16) + 1)
+    elif what == "rec_method":
+        b[24 + 8] = 2
+    elif what == "rec_stored_lens":
+        b[24 + 8] = 0
+    elif what == "rec_past_table":
+        struct.pack_into("<I", b, 24 + 4, toff)
+    elif what == "rec_count":
+        struct.pack_into("<Q", b, 16, 10 ** 6)
+    return bytes(b)
+
+
+TABLE_DAMAGE = {
+    "magic": "not a .zero archive",
+    "version": "archive version 3: this program reads version 2",
+    "block_size": "archive damaged: block size",
+    "too_short": "archive damaged: too short",
+    "footer": "archive damaged: footer (the file was cut short?)",
+    "table_position": "archive damaged: table position",
+    "table_checksum": "archive damaged: table checksum",
+    "entry_cut": "archive damaged: entry",
+    "entry_name": "archive damaged: entry name",
+    "sizes": "archive damaged: sizes",
+}
+RECORD_DAMAGE = {
+    "rec_raw_len": "archive damaged: block header",
+    "rec_method": "archive damaged: block header",
+    "rec_stored_lens": "archive damaged: block header",
+    "rec_past_table": "archive damaged: block past the table",
+    "rec_count": "archive damaged: block header cut",
+}
+
+
+def reference_error(a, tmp_path):
+    """The reference test_archive's message for these bytes (None when it accepts them)."""
+    p = tmp_path / "damaged.zero"
+    p.write_bytes(a)
+    try:
+        O.Ref.test_archive(str(p))
+        return None
+    except Exception as e:  # noqa: BLE001 -- the oracle raises with the reference's message
+        return str(e)
+
+
+@pytest.mark.parametrize("what", sorted(TABLE_DAMAGE))
+def test_table_damage(what, tmp_path):
+    a = mutate(golden("three_files.L5"), what)
+    with pytest.raises(Z.DataError) as ei:
+        Z.read_table(a)
+    assert str(ei.value) == TABLE_DAMAGE[what]
+    if O.Ref.available():
+        assert TABLE_DAMAGE[what] in reference_error(a, tmp_path)
+
+
+@pytest.mark.parametrize("what", sorted(RECORD_DAMAGE))
+def test_record_damage(what, tmp_path):
+    a = mutate(golden("three_files.L5"), what)
+    info, _ = Z.read_table(a)
+    with pytest.raises(Z.DataError) as ei:
+        Z.archive_blocks(a, info)
+    assert str(ei.value) == RECORD_DAMAGE[what]
+    if O.Ref.available() and what != "rec_count":  # (the reference reads past the table before failing there)
+        assert RECORD_DAMAGE[what] in reference_error(a, tmp_path)
+
+
+def test_reader_never_reads_outside_the_buffer():
+    """Every prefix of an archive is refused cleanly (the reader bounds each access by the length)."""
+    a = golden("three_files.L1")
+    for n in list(range(0, 64)) + [len(a) // 2, len(a) - 25, len(a) - 1]:
+        with pytest.raises(Z.DataError):
+            info, _ = Z.read_table(a[:n])
+            Z.archive_blocks(a[:n], info)
+    # random corruption of the table and footer: a DataError or a consistent parse, never a crash
+    rng = np.random.default_rng(5)
+    for _ in range(200):
+        b = bytearray(a)
+        for _ in range(3):
+            b[int(rng.integers(len(b) - 300, len(b)))] = int(rng.integers(0, 256))
+        try:
+            info, es = Z.read_table(bytes(b))
+            Z.archive_blocks(bytes(b), info)
+        except Z.DataError:
+            pass

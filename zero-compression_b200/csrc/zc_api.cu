@@ -11,21 +11,13 @@
 #include <vector>
 
 #include "../../include/zero_cuda.h"
+#include "zc_host.h"
 #include "zc_internal.cuh"
 #include "zc_kernels.h"
 
+using namespace zch;
+
 namespace {
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t n = 0;
-  template <class T> T* as() const { return static_cast<T*>(p); }
-};
-
-struct HostBuf {  // pinned staging
-  void* p = nullptr;
-  size_t n = 0;
-};
 
 __global__ void k_plain_blocks(uint64_t n, uint32_t B, uint32_t nb, uint64_t* off, uint32_t* len) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -38,7 +30,9 @@ __global__ void k_plain_blocks(uint64_t n, uint32_t B, uint32_t nb, uint64_t* of
 int depth_for_level(int level) { return level <= 1 ? 8 : level >= 9 ? 256 : 32; }
 int level_class(int level) { return level <= 1 ? 0 : level >= 9 ? 2 : 1; }
 
-void build_crc_tables(zc::CrcTables& T) {
+}  // namespace
+
+void zch::build_crc_tables(zc::CrcTables& T) {
   for (uint32_t i = 0; i < 256; ++i) {
     uint32_t r = i;
     for (int k = 0; k < 8; ++k) r = (r >> 1) ^ (0xEDB88320u & (0u - (r & 1u)));
@@ -49,43 +43,6 @@ void build_crc_tables(zc::CrcTables& T) {
   uint32_t p = 0x00800000u;  // x^8
   for (int e = 0; e < 64; ++e) { T.pow2[e] = p; p = zc::gf2_mul(p, p); }
 }
-
-// per-stage CUDA-event records of one context
-struct StageRecords {
-  struct Rec { const char* name; cudaEvent_t a, b; };
-  std::vector<cudaEvent_t> pool;
-  std::vector<Rec> pending;
-  const char* open_name = nullptr;
-  cudaEvent_t open_ev = nullptr;
-  std::map<std::string, std::pair<double, uint64_t>> totals;
-  std::vector<std::string> order;
-  cudaEvent_t get() {
-    if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
-    cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
-    return e;
-  }
-  void collect() {
-    for (const Rec& r : pending) {
-      float ms = 0;
-      cudaEventSynchronize(r.b);
-      cudaEventElapsedTime(&ms, r.a, r.b);
-      auto it = totals.find(r.name);
-      if (it == totals.end()) { order.push_back(r.name); it = totals.emplace(r.name, std::make_pair(0.0, (uint64_t)0)).first; }
-      it->second.first += ms;
-      it->second.second += 1;
-      pool.push_back(r.a);
-      pool.push_back(r.b);
-    }
-    pending.clear();
-  }
-  ~StageRecords() {
-    for (const Rec& r : pending) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
-    for (cudaEvent_t e : pool) cudaEventDestroy(e);
-  }
-};
-
-}  // namespace
 
 void zc::Stages::begin(const char* name, cudaStream_t st) {
   ++launches;
@@ -103,52 +60,7 @@ void zc::Stages::end(cudaStream_t st) {
   R->pending.push_back({R->open_name, R->open_ev, e});
 }
 
-// a captured launch sequence, replayed when a device entry point is called again with the same arguments
-struct GraphEntry {
-  int kind;
-  uint64_t key[24];
-  cudaGraphExec_t exec;
-  uint64_t launches;  // kernels in the graph
-};
-
-// per (block size, level class) launch shapes: the fill's ring and warps per CTA, the match pass's
-// compare cap (none of them changes a result byte)
-struct Shape {
-  uint32_t ring_log = 12, fill_warps = 4, cmp_cap = 16, match_tile = 1024;
-};
-
-struct zc_ctx {
-  int device = 0;
-  Shape shape[5][3];
-  bool graphs = false;
-  std::vector<GraphEntry> graph_cache;
-  cudaStream_t stream = nullptr;
-  std::string err, name;
-  uint32_t block_log = 18;
-  int level = 5;
-  zc::Stages stages;
-  StageRecords records;
-  zc::CrcTables* d_crct = nullptr;
-  // encoder scratch (sized by capacity: any block size whose blocks fit)
-  DevBuf e_tmp_pos, e_srt_pos, e_minfo, e_scnt, e_tk_seg, e_tmp_h, e_srt_h, e_tk_i, e_tk_m, e_tk_d, e_bcnt, e_lit, e_tok,
-      e_ext, e_sym, e_grp, e_bits, e_lanes, e_freq, e_lanelen, e_sinfo, e_slab;
-  // decoder scratch (likewise)
-  DevBuf d_lit, d_tok, d_sym, d_grp, d_ext, d_meta, d_tks, d_tkm, d_tkd, d_tkl, d_tot;
-  // staging for the host-pointer calls
-  DevBuf s_in, s_blk, s_out, s_meta;
-  HostBuf h_meta;
-  DevBuf work;  // the decoder fill's device work counter
-  // the host-pointer codec calls run in chunks through two stages: a chunk's copies (on cstream) overlap
-  // the other chunk's kernels (on stream)
-  struct Stage {
-    DevBuf in, blk, out, meta;
-    HostBuf h;  // descriptors up, then results down
-    cudaEvent_t ev_in = nullptr, ev_done = nullptr;
-  } pipe[2];
-  cudaStream_t cstream = nullptr;
-};
-
-namespace {
+namespace zch {
 
 int fail(zc_ctx* c, int code, const std::string& msg) {
   c->err = msg;
@@ -158,11 +70,6 @@ int cuda_fail(zc_ctx* c, cudaError_t e, const char* what) {
   c->err = std::string(what) + ": " + cudaGetErrorString(e);
   return e == cudaErrorMemoryAllocation ? ZC_E_NOMEM : ZC_E_DEVICE;
 }
-#define ZC_CUDA(call)                                  \
-  do {                                                 \
-    cudaError_t e_ = (call);                           \
-    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
-  } while (0)
 
 cudaError_t grow(DevBuf& b, size_t bytes) {
   if (bytes <= b.n && b.p) return cudaSuccess;
@@ -259,8 +166,9 @@ int check_launch(zc_ctx* c, const char* what) {
 int encode_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_off, const uint32_t* d_len, uint32_t nb,
                   uint32_t block_log, int level, uint8_t* d_methods, uint32_t* d_lens, uint32_t* d_crcs,
                   uint8_t* d_out, size_t out_cap, uint64_t* d_out_offs, uint64_t* d_total, int emit_stored,
-                  cudaStream_t st) {
+                  cudaStream_t st, const uint64_t* rec_base) {
   if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  if (rec_base && (!d_crcs || !emit_stored)) return fail(c, ZC_E_ARG, "archive records need the block CRCs");
   if (nb > enc_blocks_per_launch(block_log)) return fail(c, ZC_E_ARG, "too many blocks for one launch");
   if (int r = ensure_enc(c, nb, block_log)) return r;
   zc::EncArgs A{};
@@ -281,6 +189,7 @@ int encode_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_off, const u
   A.sinfo = c->e_sinfo.as<uint32_t>(); A.slab = c->e_slab.as<uint8_t>();
   A.out = d_out; A.out_cap = out_cap; A.out_off = d_out_offs; A.out_len = d_lens; A.out_method = d_methods;
   A.out_total = d_total; A.emit_stored = emit_stored;
+  A.rec_hdr = rec_base ? 16u : 0u; A.rec_base = rec_base; A.rec_crc = d_crcs;
   zc::CrcArgs C{};
   C.base = d_in; C.offs = d_off; C.lens = d_len; C.nb = nb; C.crc = d_crcs; C.tables = c->d_crct;
   if (!d_crcs) C.nb = 0;
@@ -313,6 +222,17 @@ int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs,
   }
   return check_launch(c, "decoder launch");
 }
+
+void plain_blocks(zc_ctx* c, uint64_t n, uint32_t B, uint32_t nb, uint64_t* d_off, uint32_t* d_len, cudaStream_t st) {
+  if (!nb) return;
+  c->stages.begin("k_plain_blocks", st);
+  k_plain_blocks<<<(nb + 255) / 256, 256, 0, st>>>(n, B, nb, d_off, d_len);
+  c->stages.end(st);
+}
+
+}  // namespace zch
+
+namespace {
 
 // Runs `body` on stream st, through a CUDA graph when graphs are on: the first call with a given key
 // captures the launches, later calls replay them.  Scratch must already be sized (a capture allocates
@@ -437,11 +357,7 @@ int compress_host(zc_ctx* c, const uint8_t* host_base, const uint64_t* in_offs, 
     ZC_CUDA(cudaEventRecord(S.ev_in, cs));
     // kernels on the compute stream once the upload is in
     ZC_CUDA(cudaStreamWaitEvent(st, S.ev_in, 0));
-    if (!in_offs) {
-      c->stages.begin("k_plain_blocks", st);
-      k_plain_blocks<<<(k + 255) / 256, 256, 0, st>>>(span, B, k, d_off, d_len);
-      c->stages.end(st);
-    }
+    if (!in_offs) plain_blocks(c, span, B, k, d_off, d_len, st);
     uint8_t* m = S.meta.as<uint8_t>();
     uint64_t* d_poff = reinterpret_cast<uint64_t*>(m);
     uint64_t* d_total = d_poff + k;
@@ -511,7 +427,8 @@ void zc_close(zc_ctx* c) {
   for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_minfo, &c->e_scnt, &c->e_tk_seg, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
                     &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
                     &c->e_bits, &c->e_lanes, &c->e_freq, &c->e_lanelen, &c->e_sinfo, &c->e_slab, &c->d_lit, &c->d_tok,
-                    &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta, &c->work})
+                    &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta, &c->work,
+                    &c->a_desc, &c->a_work, &c->a_in, &c->a_out})
     release(*b);
   if (c->h_meta.p) cudaFreeHost(c->h_meta.p);
   for (auto& S : c->pipe) {

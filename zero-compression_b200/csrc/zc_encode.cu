@@ -923,7 +923,7 @@ __global__ void __launch_bounds__(1024) k_enc_scan(EncArgs A) {
   uint64_t sum = 0;
   for (uint32_t b = b0; b < b1; ++b) {
     const uint32_t* c = A.bcnt + b * 8;
-    sum += c[6] ? c[5] : (A.emit_stored ? A.in_len[b] : 0u);
+    sum += A.rec_hdr + (c[6] ? c[5] : (A.emit_stored ? A.in_len[b] : 0u));
   }
   __shared__ uint64_t ws[32];
   uint64_t incl = sum;
@@ -945,11 +945,12 @@ __global__ void __launch_bounds__(1024) k_enc_scan(EncArgs A) {
     ws[tid] = x - v;
   }
   __syncthreads();
-  uint64_t off = ws[tid >> 5] + incl - sum;
+  uint64_t off = (A.rec_base ? *A.rec_base : 0ull) + ws[tid >> 5] + incl - sum;
   for (uint32_t b = b0; b < b1; ++b) {
     const uint32_t* c = A.bcnt + b * 8;
     const uint32_t method = c[6];
     const uint32_t len = method ? c[5] : A.in_len[b];
+    off += A.rec_hdr;
     A.out_off[b] = off;
     A.out_len[b] = len;
     A.out_method[b] = (uint8_t)method;
@@ -967,6 +968,11 @@ __global__ void __launch_bounds__(256) k_enc_emit(EncArgs A) {
   if (off + len > A.out_cap) return;  // (the host checks out_total against out_cap)
   const uint8_t* s = method ? A.slab + (size_t)b * A.B : A.in + A.in_off[b];
   uint8_t* d = A.out + off;
+  if (A.rec_hdr && threadIdx.x < 16) {  // the record header just before the body (off >= 16 here)
+    const uint32_t t = threadIdx.x, w = t >> 2, sh = 8u * (t & 3u);
+    const uint32_t v = w == 0 ? A.in_len[b] : w == 1 ? len : w == 2 ? method : A.rec_crc[b];
+    d[(int)t - 16] = (w == 2 && t != 8) ? 0 : (uint8_t)(v >> sh);
+  }
   uint32_t i = 0;
   if ((((uintptr_t)d ^ (uintptr_t)s) & 15u) == 0) {
     const uint32_t head = min(len, (uint32_t)((16u - ((uintptr_t)d & 15u)) & 15u));

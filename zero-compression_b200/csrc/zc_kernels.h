@@ -93,8 +93,14 @@ struct EncArgs {
   uint64_t* out_off;              // per block
   uint32_t* out_len;              // per block: payload length (raw length when stored)
   uint8_t* out_method;            // per block
-  uint64_t* out_total;            // device u64: bytes written to out
+  uint64_t* out_total;            // device u64: bytes written to out (record mode: the end of the last record)
   int emit_stored;                // 1: copy stored blocks' raw bytes into out as well
+  // archive record mode (rec_hdr = 16): every body is preceded by its block record header {u32 raw_len,
+  // u32 comp_len, u8 method, 3 zero bytes, u32 crc} (src/archive.h:389-403), the first record at
+  // *rec_base; rec_crc holds the blocks' CRCs (written by the first stage).  rec_hdr = 0: bodies from 0.
+  uint32_t rec_hdr;
+  const uint64_t* rec_base;
+  const uint32_t* rec_crc;
 };
 
 // lane scratch layout per block: stream s starts at lane_base(s), each of its 64 lanes has lane_cap(s)

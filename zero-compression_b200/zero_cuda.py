@@ -91,6 +91,16 @@ def lib():
         L.zc_set_shape.argtypes = [_vp, C.c_uint32, C.c_int, C.POINTER(Shape)]
         L.zc_autotune.argtypes = [_vp, _vp, C.c_size_t, C.c_uint32, C.c_int, C.POINTER(Shape)]
         L.zc_profile_stages.argtypes = [_vp, C.c_uint32, _vp, _vp, _vp, _u32p]
+        L.zc_archive_bound.argtypes = [_vp, C.c_uint32, C.c_uint32]
+        L.zc_archive_bound.restype = C.c_uint64
+        L.zc_archive_write_device.argtypes = [_vp, _vp, C.c_uint32, C.c_int, _vp, C.c_uint32, _vp, C.c_uint64, _vp,
+                                              _vp, _vp]
+        L.zc_archive_write.argtypes = [_vp, _vp, C.c_uint32, C.c_int, _vp, C.c_uint32, _vp, C.c_uint64, _u64p]
+        L.zc_archive_read_table.argtypes = [_vp, C.c_uint64, C.POINTER(ArchiveInfo), _vp, C.c_uint32, C.c_char_p,
+                                            C.c_size_t]
+        L.zc_archive_blocks.argtypes = [_vp, C.c_uint64, C.POINTER(ArchiveInfo), _vp, _vp, _vp, _vp, _vp, C.c_char_p,
+                                        C.c_size_t]
+        L.zc_archive_extract.argtypes = [_vp, _vp, C.c_uint64, _vp, C.c_uint64]
         _lib = L
     return _lib
 
@@ -102,6 +112,101 @@ class Shape(C.Structure):
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+class ArchiveInfo(C.Structure):
+    """zc_archive_info: an archive's layout, from its header, footer and table."""
+    _fields_ = [("block_log", C.c_uint32), ("n_entries", C.c_uint32), ("total_raw", C.c_uint64),
+                ("n_blocks", C.c_uint64), ("table_off", C.c_uint64), ("table_len", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+class _Entry(C.Structure):  # zc_entry
+    _fields_ = [("name", C.c_void_p), ("name_len", C.c_uint32), ("is_dir", C.c_uint32), ("size", C.c_uint64),
+                ("mtime", C.c_int64), ("attr", C.c_uint32), ("crc", C.c_uint32)]
+
+
+@dataclass
+class ArchiveEntry:
+    """One entry of an archive's table (src/archive.h:139-147): a file's bytes follow the previous
+    file's in the solid stream; a folder has none."""
+    name: str
+    size: int = 0
+    mtime: int = 0
+    attr: int = 0
+    is_dir: bool = False
+    crc: int = 0
+
+
+def _c_entries(entries):
+    """zc_entry array for `entries` (and the name buffers it points into, to keep alive)."""
+    arr = (_Entry * max(len(entries), 1))()
+    keep = []
+    for i, e in enumerate(entries):
+        nm = e.name.encode("utf-8", "surrogateescape") if isinstance(e.name, str) else bytes(e.name)
+        buf = C.create_string_buffer(nm, max(len(nm), 1))
+        keep.append(buf)
+        arr[i].name = C.cast(buf, C.c_void_p)
+        arr[i].name_len = len(nm)
+        arr[i].is_dir = 1 if e.is_dir else 0
+        arr[i].size = e.size
+        arr[i].mtime = e.mtime
+        arr[i].attr = e.attr
+        arr[i].crc = e.crc
+    return arr, keep
+
+
+def archive_bound(entries, block_log):
+    """The largest archive zc_archive_write can produce for these entries (0 for invalid ones)."""
+    arr, _keep = _c_entries(entries)
+    return int(lib().zc_archive_bound(arr, len(entries), block_log))
+
+
+def read_table(arch):
+    """An archive's header, footer and entry table, checked as read_info does (src/archive.h:451-495):
+    -> (info dict, [ArchiveEntry]).  Host-only (no GPU).  Raises DataError for a damaged archive."""
+    a = _as_u8(arch)
+    info = ArchiveInfo()
+    msg = C.create_string_buffer(512)
+    rc = lib().zc_archive_read_table(_ptr(a), a.size, C.byref(info), None, 0, msg, 512)
+    if rc:
+        raise DataError(msg.value.decode(errors="replace")) if rc == ZC_E_DATA else ArgError("bad arguments")
+    n = info.n_entries
+    arr = (_Entry * max(n, 1))()
+    lib().zc_archive_read_table(_ptr(a), a.size, C.byref(info), arr, n, msg, 512)
+    out = []
+    for i in range(n):
+        e = arr[i]
+        name = C.string_at(e.name, e.name_len) if e.name_len else b""
+        out.append(ArchiveEntry(name.decode("utf-8", "surrogateescape"), int(e.size), int(e.mtime), int(e.attr),
+                                bool(e.is_dir), int(e.crc)))
+    return info.as_dict(), out
+
+
+def archive_blocks(arch, info=None):
+    """The block records of an archive (src/archive.h:566-586), checked as read_blocks does: a dict of
+    arrays offs (where each body starts in arch), comp_lens, methods, raw_lens, crcs.  Host-only."""
+    a = _as_u8(arch)
+    if info is None:
+        info, _ = read_table(arch)
+    I = ArchiveInfo(**info)
+    nb = int(I.n_blocks)
+    if nb > a.size // 16:
+        raise DataError("archive damaged: block header cut")
+    offs = np.zeros(max(nb, 1), np.uint64)
+    clens = np.zeros(max(nb, 1), np.uint32)
+    methods = np.zeros(max(nb, 1), np.uint8)
+    rlens = np.zeros(max(nb, 1), np.uint32)
+    crcs = np.zeros(max(nb, 1), np.uint32)
+    msg = C.create_string_buffer(512)
+    rc = lib().zc_archive_blocks(_ptr(a), a.size, C.byref(I), _ptr(offs), _ptr(clens), _ptr(methods), _ptr(rlens),
+                                 _ptr(crcs), msg, 512)
+    if rc:
+        raise DataError(msg.value.decode(errors="replace")) if rc == ZC_E_DATA else ArgError("bad arguments")
+    return {"offs": offs[:nb], "comp_lens": clens[:nb], "methods": methods[:nb], "raw_lens": rlens[:nb],
+            "crcs": crcs[:nb]}
 
 
 def _ptr(a):
@@ -320,6 +425,43 @@ class CudaCodec:
         self._check(lib().zc_decompress_device(
             self._ctx, _dp(d_comp), _dp(d_comp_offs), _dp(d_comp_lens), _dp(d_methods), _dp(d_raw_lens), nb,
             block_log, _dp(d_out), _dp(d_out_offs), _dp(d_crcs), _dp(d_err), stream or None))
+
+    # -- whole archives (include/zero_cuda.h: zc_archive_*)
+    def archive_write(self, solid, entries, block_log, level=None):
+        """The .zero archive of `solid` (the files' bytes in entry order) with table `entries`, built on
+        the GPU (compress_archive, src/archive.h:334-441) -> bytes.  Sets each entry's crc."""
+        a = _as_u8(solid)
+        if a.size == 0:
+            a = np.zeros(1, np.uint8)
+        arr, _keep = _c_entries(entries)
+        cap = archive_bound(entries, block_log)
+        if not cap:
+            raise ArgError("invalid entries or block size")
+        out = np.empty(cap, np.uint8)
+        n = C.c_uint64()
+        self._check(lib().zc_archive_write(self._ctx, _ptr(a), block_log, self.level if level is None else level,
+                                           arr, len(entries), _ptr(out), out.size, C.byref(n)))
+        for i, e in enumerate(entries):
+            e.crc = int(arr[i].crc)
+        return out[: n.value].tobytes()
+
+    def archive_write_device(self, d_solid, entries, block_log, d_out, d_len, d_entry_crcs=None, stream=0,
+                             level=None, out_cap=None):
+        """zc_archive_write_device: device solid stream -> the archive in d_out, its length in d_len."""
+        arr, _keep = _c_entries(entries)
+        self._check(lib().zc_archive_write_device(
+            self._ctx, _dp(d_solid), block_log, self.level if level is None else level, arr, len(entries),
+            _dp(d_out), out_cap if out_cap is not None else d_out.numel(), _dp(d_len), _dp(d_entry_crcs),
+            stream or None))
+
+    def archive_extract(self, arch, test=False):
+        """Decodes and checks every block and file of an archive on the GPU (read_blocks + extract_archive /
+        test_archive, src/archive.h:566-635, 747-785) -> the solid stream (None when test)."""
+        a = _as_u8(arch)
+        info, _ = read_table(a)
+        out = None if test else np.empty(max(info["total_raw"], 1), np.uint8)
+        self._check(lib().zc_archive_extract(self._ctx, _ptr(a), a.size, _ptr(out), 0 if out is None else out.size))
+        return None if test else out[: info["total_raw"]].tobytes()
 
 
 def _dp(x):
