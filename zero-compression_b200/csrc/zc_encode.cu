@@ -626,6 +626,8 @@ __global__ void __launch_bounds__(256, 8) k_enc_parse(EncArgs A) {  // (8 CTAs a
 }
 
 // ---------------------------------------------------------------- 4. tokens -> streams
+constexpr uint32_t kWarpCopyRun = 32;
+
 __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
   const uint32_t w = threadIdx.x >> 5, lane = lane_id();
   const uint32_t b = blockIdx.x * 4 + w;
@@ -708,10 +710,18 @@ __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
     if (lane < 24) win[w][lane] = lane == 0 ? carry : 0u;
     __syncwarp();
     wbase += 32ull * full;
-    // literals before each token
+    // literals before each token: a lane copies its own short run; runs of kWarpCopyRun bytes or more
+    // (a long incompressible stretch) are copied by the whole warp, one after another
     const uint32_t lincl = warp_incl_scan(L);
     const uint32_t lik = li + lincl - L;
-    for (uint32_t k = 0; k < L; ++k) lit[lik + k] = src[opk + k];
+    const bool longrun = L >= kWarpCopyRun;
+    if (!longrun)
+      for (uint32_t k = 0; k < L; ++k) lit[lik + k] = src[opk + k];
+    for (unsigned lb = __ballot_sync(kFull, longrun); lb; lb &= lb - 1) {
+      const uint32_t q = (uint32_t)__ffs(lb) - 1u;
+      const uint32_t qL = __shfl_sync(kFull, L, q), qd = __shfl_sync(kFull, lik, q), qs = __shfl_sync(kFull, opk, q);
+      for (uint32_t k = lane; k < qL; k += 32) lit[qd + k] = src[qs + k];
+    }
     li += __shfl_sync(kFull, lincl, 31);
     ei += __shfl_sync(kFull, xincl, 31);
     op = __shfl_sync(kFull, endk, c - 1);
@@ -745,6 +755,8 @@ __device__ __forceinline__ uint32_t stream_len(const EncArgs& A, uint32_t b, uin
   return s == 0 ? c[1] : s == 2 ? c[2] : s == 4 ? c[4] : c[0];
 }
 
+constexpr uint32_t kRansChunk = 4096;  // symbols staged per round: 64 per lane
+
 __global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
   const uint32_t b = blockIdx.x, s = blockIdx.y, k = threadIdx.x, g = b * 5 + s;
   const uint32_t ns = stream_len(A, b, s);
@@ -754,7 +766,8 @@ __global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
     return;
   }
   const uint8_t* sym = stream_syms(A, b, s);
-  __shared__ uint32_t hist[256], freq[256], cum[256], red[3];
+  __shared__ uint32_t hist[256], fc[256], red[3];   // fc: freq | cum << 16
+  __shared__ __align__(16) uint8_t stage[kRansChunk];
   for (uint32_t i = k; i < 256; i += 64) hist[i] = 0;
   __syncthreads();
   for (uint32_t i = k; i < ns; i += 64) atomicAdd(&hist[sym[i]], 1u);
@@ -809,8 +822,7 @@ __global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
     uint32_t c0 = warp_incl_scan(tot) - tot;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      freq[k * 8 + q] = f[q];
-      cum[k * 8 + q] = c0;
+      fc[k * 8 + q] = f[q] | c0 << 16;
       A.freq[(size_t)g * 256 + k * 8 + q] = (uint16_t)f[q];
       c0 += f[q];
     }
@@ -822,12 +834,30 @@ __global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
   uint8_t* end = A.lanes + (size_t)b * lanes_per_block(A.B) + lane_base(A.B, s) + (size_t)(k + 1) * LC;
   uint8_t* ptr = end;
   uint32_t x = kRansLow;
-  if (k < ns) {
-    for (int64_t i = k + (int64_t)((ns - 1 - k) / kLanes) * kLanes; i >= 0; i -= kLanes) {
-      const uint32_t c = sym[i], f = freq[c];
-      const uint32_t xmax = f << (23 - kScaleBits + 8);
-      while (x >= xmax) { *--ptr = (uint8_t)x; x >>= 8; }
-      x = ((x / f) << kScaleBits) + (x % f) + cum[c];
+  // The stream in chunks of kRansChunk symbols (a whole number of rounds of the 64 lanes), last chunk
+  // first: the CTA stages a chunk in shared memory with coalesced loads, then lane k codes its symbols
+  // c0 + k + 64 j of it, j descending -- the order of the whole-stream loop, without a global load on
+  // the state's dependency chain.
+  const bool al4 = ((uintptr_t)sym & 3u) == 0;
+  for (int32_t ch = (int32_t)((ns - 1) / kRansChunk); ch >= 0; --ch) {
+    const uint32_t c0 = (uint32_t)ch * kRansChunk, cn = min(kRansChunk, ns - c0);
+    __syncthreads();  // (the previous chunk is coded)
+    uint32_t t0 = 0;
+    if (al4) {
+      const uint32_t n4 = cn >> 2;
+      for (uint32_t t = k; t < n4; t += kLanes)
+        reinterpret_cast<uint32_t*>(stage)[t] = reinterpret_cast<const uint32_t*>(sym + c0)[t];
+      t0 = n4 << 2;
+    }
+    for (uint32_t t = t0 + k; t < cn; t += kLanes) stage[t] = sym[c0 + t];
+    __syncthreads();
+    if (k < cn) {
+      for (int32_t t = (int32_t)(k + (cn - 1 - k) / kLanes * kLanes); t >= 0; t -= (int32_t)kLanes) {
+        const uint32_t e = fc[stage[t]], f = e & 0xFFFFu;
+        const uint32_t xmax = f << (23 - kScaleBits + 8);
+        while (x >= xmax) { *--ptr = (uint8_t)x; x >>= 8; }
+        x = ((x / f) << kScaleBits) + (x % f) + (e >> 16);
+      }
     }
   }
   ptr -= 4;
