@@ -530,6 +530,121 @@ def run_batched(args):
     return 0 if plain["bit_exact"] and batched["bit_exact"] else 1
 
 
+def run_sweep(args):
+    """The LZ-mix sweep: 1 GiB of lz_mix at block 16/18/20 x level 1/5/9, and 2 GiB of uniform random bytes
+    at block 16/18/20 (every block stored).  Per cell, device-resident: compress and decompress GB/s (CUDA
+    events, mean of the timed steps), the ratio, the round trip bit-exact, and the first blocks' payloads
+    compared byte for byte with the reference CPU codec's (oracle/_ref, when present)."""
+    import numpy as np
+    import torch
+    import zero_cuda as Z
+    import datagen as G
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    have_ref = O.Ref.available()
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    cells = []
+    plan = [("lz_mix", args.size_mib << 20, bl, lv) for bl in (16, 18, 20) for lv in (1, 5, 9)]
+    plan += [("random", 2 * (args.size_mib << 20), bl, 5) for bl in (16, 18, 20)]
+    data_cache = {}
+    with ClockSampler(local) as clk:
+        for kind, n, bl, lv in plan:
+            B = 1 << bl
+            nb = (n + B - 1) // B
+            key = (kind, n, bl)
+            if key not in data_cache:
+                data_cache.clear()
+                data_cache[key] = make_data(n, bl, 1000) if kind == "lz_mix" else G.random_bytes(n, 77)
+            host = data_cache[key]
+            codec = Z.CudaCodec(level=lv, device=local)
+            per = codec.batch_bytes(bl) // B
+            dper = codec.batch_bytes_decode(bl) // B
+            d_in = torch.zeros(n + 64, dtype=torch.uint8, device=dev)
+            d_in[:n].copy_(torch.from_numpy(host))
+            offs = torch.arange(nb, dtype=torch.int64, device=dev) * B
+            lens = torch.clamp(n - offs, max=B).to(torch.int32)
+            d_out = torch.zeros(n + 64, dtype=torch.uint8, device=dev)
+            d_dec = torch.zeros(n + 64, dtype=torch.uint8, device=dev)
+            methods = torch.zeros(nb, dtype=torch.uint8, device=dev)
+            clens = torch.zeros(nb, dtype=torch.int32, device=dev)
+            crcs = torch.zeros(nb, dtype=torch.int32, device=dev)
+            dcrcs = torch.zeros(nb, dtype=torch.int32, device=dev)
+            errs = torch.zeros(nb, dtype=torch.int32, device=dev)
+            ooffs = torch.zeros(nb, dtype=torch.int64, device=dev)
+            goffs = torch.zeros(nb, dtype=torch.int64, device=dev)
+            chunks = [(b0, min(per, nb - b0)) for b0 in range(0, nb, per)]
+            totals = torch.zeros(len(chunks), dtype=torch.int64, device=dev)
+            base = torch.tensor([b0 * B for b0, k in chunks for _ in range(k)], dtype=torch.int64, device=dev)
+
+            def compress():
+                for ci, (b0, k) in enumerate(chunks):
+                    o = b0 * B
+                    codec.compress_device(d_in, offs[b0:], lens[b0:], k, bl, methods[b0:], clens[b0:], crcs[b0:],
+                                          d_out[o:o + k * B + 64], ooffs[b0:], totals[ci:], stream=sh)
+                with torch.cuda.stream(stream):
+                    torch.add(ooffs, base, out=goffs)
+
+            def decompress():
+                for b0 in range(0, nb, dper):
+                    k = min(dper, nb - b0)
+                    codec.decompress_device(d_out, goffs[b0:], clens[b0:], methods[b0:], lens[b0:], k, bl, d_dec,
+                                            offs[b0:], dcrcs[b0:], errs[b0:], stream=sh)
+
+            for _ in range(args.warmup):
+                compress()
+                decompress()
+            torch.cuda.synchronize(dev)
+            ev = [_events(2) for _ in range(args.steps)]
+            with torch.cuda.stream(stream):
+                for i in range(args.steps):
+                    ev[i][0][0].record(stream); compress(); ev[i][0][1].record(stream)
+                    ev[i][1][0].record(stream); decompress(); ev[i][1][1].record(stream)
+            torch.cuda.synchronize(dev)
+            tc = sum(e[0][0].elapsed_time(e[0][1]) for e in ev) / args.steps
+            td = sum(e[1][0].elapsed_time(e[1][1]) for e in ev) / args.steps
+            ok = bool(torch.equal(d_dec[:n], d_in[:n])) and bool(torch.equal(dcrcs, crcs)) and not errs.any()
+            comp = int(clens.sum().item())
+            cell = {"data": kind, "bytes": n, "block_log": bl, "level": lv, "compress_gbs": round(n / tc / 1e6, 3),
+                    "decompress_gbs": round(n / td / 1e6, 3), "round_trip_gbs": round(n / (tc + td) / 1e6, 3),
+                    "ratio": round(comp / n, 5), "stored_blocks": int((methods == 0).sum().item()), "bit_exact": ok}
+            if have_ref:
+                k = min(nb, max(4, (8 << 20) >> bl))
+                rm, rl, rp = O.Ref.cpu_compress(host[:k * B], bl, O.depth_for_level(lv))
+                gm = methods[:k].cpu().numpy()
+                gl = clens[:k].cpu().numpy()
+                go = goffs[:k].cpu().numpy()
+                span = d_out[:int(go[-1]) + int(gl[-1])].cpu().numpy()
+                same = bool(np.array_equal(gm, np.asarray(rm, np.uint8)))
+                for b in range(k):
+                    if same and gm[b]:
+                        same = span[int(go[b]):int(go[b]) + int(gl[b])].tobytes() == bytes(rp[b])
+                cell["payloads_equal_reference"] = {"blocks": k, "equal": same}
+                ok = ok and same
+            cells.append(cell)
+            print(json.dumps(cell), file=sys.stderr, flush=True)
+            codec.close()
+            del d_in, d_out, d_dec
+            torch.cuda.empty_cache()
+    head = next(c for c in cells if c["data"] == "lz_mix" and c["block_log"] == 18 and c["level"] == 5)
+    all_ok = all(c["bit_exact"] and c.get("payloads_equal_reference", {"equal": True})["equal"] for c in cells)
+    line = {"metric": METRIC, "value": head["round_trip_gbs"], "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "dtype": "u8",
+            "data": "synthetic (seeded lz_mix and uniform random generators)",
+            "config": {"workload": f"sweep: lz_mix {args.size_mib} MiB at block 16/18/20 x level 1/5/9, random "
+                                   f"{2 * args.size_mib} MiB at block 16/18/20 (level 5); value = the block 18 "
+                                   f"level 5 cell's round trip",
+                       "l2_flush": "none needed: every input is larger than the 126 MB L2"},
+            "cells": cells, "bit_exact": all_ok, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0 if all_ok else 1
+
+
 def run_archive(args):
     """Whole-archive workload: the many-file set of the batched config written as one .zero archive whose
     records, file CRCs (over each file's span, across blocks), entry table and footer are assembled on
@@ -628,6 +743,15 @@ def run_archive(args):
           and np.array_equal(h_back[:total], hv[:total])
           and [int(x) & 0xFFFFFFFF for x in d_ecrc.cpu().tolist()] == [int(arr[i].crc) for i in range(ne)])
     info, _ = Z.read_table(dev_arch)
+    # the dominant kernel of one (profiled) write; algorithmic bytes of a write: raw read + archive written
+    peak, peak_kind = peaks()
+    dom_name, (dom_ms, dom_n) = max(stages.items(), key=lambda kv: kv[1][0])
+    alg = total + alen
+    roof = {"bound": "hbm", "kernel": dom_name, "achieved": round(alg / (dom_ms * 1e-3) / GB, 2), "peak": peak,
+            "unit": "GB/s", "frac": round(alg / (dom_ms * 1e-3) / GB / peak, 4), "traffic": None,
+            "peak_source": peak_kind, "algorithmic_bytes_per_launch": int(alg / max(1, dom_n)),
+            "avg_launch_ms": round(dom_ms / max(1, dom_n), 4),
+            "pipeline_frac": round(alg / (t_w * 1e-3) / GB / peak, 4)}
     line = {"metric": METRIC, "value": round(total / t_w / 1e6, 3), "unit": "GB/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_w, 3), "higher_is_better": True,
             "scaling": "weak", "dtype": "u8", "data": "synthetic (seeded per-file generators)",
@@ -637,7 +761,7 @@ def run_archive(args):
                                    f"the GPU (records, file CRCs, table, footer)",
                        "blocks": int(info["n_blocks"]), "bytes": total, "archive_bytes": alen,
                        "l2_flush": "none needed: input larger than the 126 MB L2"},
-            "ratio": round(alen / total, 5), "bit_exact": bool(ok), "gpu_launches": launches,
+            "ratio": round(alen / total, 5), "bit_exact": bool(ok), "gpu_launches": launches, "roofline": roof,
             "stages_ms_per_step": {k: round(v[0], 4) for k, v in stages.items()},
             "e2e": {"value": round(total / t_e / 1e9, 4), "unit": "GB/s",
                     "h2d_bytes_per_step": int(total + alen), "d2h_bytes_per_step": int(alen + total),
@@ -916,9 +1040,10 @@ def main():
     ap.add_argument("--level", type=int, default=None, help="default 5; 9 for --config decode")
     ap.add_argument("--size-mib", type=int, default=None, help="default 1024; 8192 for --config decode")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--config", choices=["lz", "batched", "decode", "serve", "archive"], default="lz",
+    ap.add_argument("--config", choices=["lz", "batched", "decode", "serve", "archive", "sweep"], default="lz",
                     help="lz: the headline round trip; batched: many files, plain vs batched; decode: extract-heavy; "
-                         "serve: the request loop; archive: whole .zero archives of many files")
+                         "serve: the request loop; archive: whole .zero archives of many files; sweep: lz_mix at "
+                         "block 16/18/20 x level 1/5/9 and random bytes")
     ap.add_argument("--files", type=int, default=10000)
     ap.add_argument("--max-file-kib", type=int, default=1024)
     ap.add_argument("--pool", type=int, default=48, help="serve: distinct files the jobs draw from")
@@ -944,6 +1069,8 @@ def main():
         return run_serve(args)
     if args.config == "archive":
         return run_archive(args)
+    if args.config == "sweep":
+        return run_sweep(args)
     return run_ours(args)
 
 

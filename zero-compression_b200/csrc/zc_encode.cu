@@ -766,7 +766,8 @@ __global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
     return;
   }
   const uint8_t* sym = stream_syms(A, b, s);
-  __shared__ uint32_t hist[256], fc[256], red[3];   // fc: freq | cum << 16
+  // per symbol: fc = freq | cum << 13 | (ceil(log2 freq) - 1) << 25, rcp = ceil(2^(31 + ceil(log2 freq)) / freq)
+  __shared__ uint32_t hist[256], fc[256], rcp[256], red[3];
   __shared__ __align__(16) uint8_t stage[kRansChunk];
   for (uint32_t i = k; i < 256; i += 64) hist[i] = 0;
   __syncthreads();
@@ -822,7 +823,9 @@ __global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
     uint32_t c0 = warp_incl_scan(tot) - tot;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      fc[k * 8 + q] = f[q] | c0 << 16;
+      const uint32_t sl = f[q] > 1 ? 32u - __clz(f[q] - 1u) : 1u;  // ceil(log2 f)
+      fc[k * 8 + q] = f[q] | c0 << 13 | (sl - 1u) << 25;
+      rcp[k * 8 + q] = f[q] > 1 ? (uint32_t)(((1ull << (31 + sl)) + f[q] - 1u) / f[q]) : 0u;
       A.freq[(size_t)g * 256 + k * 8 + q] = (uint16_t)f[q];
       c0 += f[q];
     }
@@ -852,11 +855,16 @@ __global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
     for (uint32_t t = t0 + k; t < cn; t += kLanes) stage[t] = sym[c0 + t];
     __syncthreads();
     if (k < cn) {
+      // x' = (x / f) * 4096 + x % f + cum = x + cum + q * (4096 - f), with q = x / f by an exact
+      // reciprocal: for x < 2^31 and s = ceil(log2 f), floor(x * ceil(2^(31+s) / f) / 2^(31+s)) = x / f
+      // (the product's error is below x / 2^(31+s) < 2^-s <= 1/f, less than the gap to the next integer)
       for (int32_t t = (int32_t)(k + (cn - 1 - k) / kLanes * kLanes); t >= 0; t -= (int32_t)kLanes) {
-        const uint32_t e = fc[stage[t]], f = e & 0xFFFFu;
+        const uint32_t c = stage[t], e = fc[c], m = rcp[c];
+        const uint32_t f = e & 0x1FFFu;
         const uint32_t xmax = f << (23 - kScaleBits + 8);
         while (x >= xmax) { *--ptr = (uint8_t)x; x >>= 8; }
-        x = ((x / f) << kScaleBits) + (x % f) + (e >> 16);
+        const uint32_t q = f == 1 ? x : __umulhi(x, m) >> (e >> 25);
+        x += ((e >> 13) & 0xFFFu) + q * (kScale - f);
       }
     }
   }
