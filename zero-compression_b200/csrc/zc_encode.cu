@@ -628,6 +628,30 @@ __global__ void __launch_bounds__(256, 8) k_enc_parse(EncArgs A) {  // (8 CTAs a
 // ---------------------------------------------------------------- 4. tokens -> streams
 constexpr uint32_t kWarpCopyRun = 32;
 
+// n bytes from src, a range of the codec's input (16-byte aligned, 64 readable bytes after its end), to
+// dst by the 32 lanes of a warp: 4-byte words stored aligned at dst, each built by a funnel shift from
+// the two aligned input words that cover it (those may reach a few bytes past the range, into the
+// input's slack, never before the input's start), four words a lane in flight.
+__device__ __forceinline__ void warp_copy_in(uint8_t* dst, const uint8_t* src, uint32_t n, uint32_t lane) {
+  const uint32_t head = min(n, (4u - ((uint32_t)(uintptr_t)dst & 3u)) & 3u);
+  if (lane < head) dst[lane] = src[lane];
+  dst += head;
+  src += head;
+  n -= head;
+  const uint32_t nw = n >> 2, sh = (uint32_t)(uintptr_t)src & 3u;
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(src - sh);
+  uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+  if (sh) {
+#pragma unroll 4
+    for (uint32_t w = lane; w < nw; w += 32) d[w] = __funnelshift_r(s[w], s[w + 1], 8u * sh);
+  } else {
+#pragma unroll 4
+    for (uint32_t w = lane; w < nw; w += 32) d[w] = s[w];
+  }
+  const uint32_t t = nw << 2;
+  if (lane < n - t) dst[t + lane] = src[t + lane];
+}
+
 __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
   const uint32_t w = threadIdx.x >> 5, lane = lane_id();
   const uint32_t b = blockIdx.x * 4 + w;
@@ -650,11 +674,15 @@ __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
   uint32_t op = 0, gstart = 0, gt = 0, ng = 0, ei = 0, li = 0;
   uint64_t bp = 0, wbase = 0;
   uint32_t r0 = 1, r1 = 4, r2 = 8, l0 = 1, l1 = 4, l2 = 8;
+  // tokens 32 at a time; the next 32 are loaded while these are coded
+  uint32_t ni = 0, nm = 4, nd = 1;
+  if (lane < nt) { ni = TI[lane]; nm = TM[lane]; nd = TD[lane]; }
   for (uint32_t t0 = 0; t0 < nt; t0 += 32) {
     const uint32_t c = min(32u, nt - t0);
     const uint32_t q = t0 + lane;
     const bool on = lane < c;
-    const uint32_t i = on ? TI[q] : 0u, m = on ? TM[q] : 4u, d = on ? TD[q] : 1u;
+    const uint32_t i = ni, m = nm, d = nd;
+    if (q + 32 < nt) { ni = TI[q + 32]; nm = TM[q + 32]; nd = TD[q + 32]; } else { ni = 0; nm = 4; nd = 1; }
     const uint32_t endk = i + m;
     const uint32_t prev_end = __shfl_up_sync(kFull, endk, 1);
     const uint32_t opk = lane == 0 ? op : prev_end;
@@ -720,7 +748,7 @@ __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
     for (unsigned lb = __ballot_sync(kFull, longrun); lb; lb &= lb - 1) {
       const uint32_t q = (uint32_t)__ffs(lb) - 1u;
       const uint32_t qL = __shfl_sync(kFull, L, q), qd = __shfl_sync(kFull, lik, q), qs = __shfl_sync(kFull, opk, q);
-      for (uint32_t k = lane; k < qL; k += 32) lit[qd + k] = src[qs + k];
+      warp_copy_in(lit + qd, src + qs, qL, lane);
     }
     li += __shfl_sync(kFull, lincl, 31);
     ei += __shfl_sync(kFull, xincl, 31);
@@ -728,7 +756,7 @@ __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
   }
   if (gt && lane == 0) grp[ng] = (uint8_t)gt;
   if (gt) ++ng;
-  for (uint32_t k = op + lane; k < n; k += 32) lit[li + (k - op)] = src[k];
+  warp_copy_in(lit + li, src + op, n - op, lane);
   li += n - op;
   if (bp > wbase && lane == 0) bitw[wbase >> 5] = win[w][0];
   if (lane == 0) {
