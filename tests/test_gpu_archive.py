@@ -189,8 +189,8 @@ def python_archive(codec, solid, es, block_log, level):
 
 
 def test_archive_over_several_encoder_launches(codec):
-    """1 GiB + 300 KiB at block 16: two encoder launches, the second's records placed after the first's
-    on the device; files straddle the launch boundary."""
+    """1 GiB + 300 KiB at block 16: the host write streams it in four chunks (128, 512, 384 MiB and the
+    rest), each chunk's records coming down while the next is coded; files straddle the chunks."""
     import datagen as G
     n = (1 << 30) + 300 * 1024
     solid = np.concatenate([G.lz_mix(n - 600 * 1024, 16, 21), G.random_bytes(300 * 1024, 22),
@@ -205,4 +205,17 @@ def test_archive_over_several_encoder_launches(codec):
     info, back = Z.read_table(got)
     assert info["n_blocks"] == (n + 65535) >> 16 > 16384
     assert [e.crc for e in back] == [e.crc for e in es]
+    # the host calls stream through two stages in 128 / 512 MiB chunks: files straddle the chunks too
+    assert codec.archive_extract(got) == solid
     assert codec.archive_extract(got, test=True) is None
+    # the device form: two encoder launches, the second's records placed after the first's on the device
+    import torch
+    d_solid = torch.zeros(n + 64, dtype=torch.uint8, device="cuda")
+    d_solid[:n] = torch.frombuffer(bytearray(solid), dtype=torch.uint8).cuda()
+    cap = Z.archive_bound(es, 16)
+    d_out = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    d_len = torch.zeros(1, dtype=torch.int64, device="cuda")
+    codec.archive_write_device(d_solid, es, 16, d_out, d_len, level=1)
+    torch.cuda.synchronize()
+    assert int(d_len.item()) == len(got)
+    assert d_out[:len(got)].cpu().numpy().tobytes() == got

@@ -223,6 +223,13 @@ int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs,
   return check_launch(c, "decoder launch");
 }
 
+// blocks in chunk `i` of a host-pointer call: 128 MiB first (so the first kernels start early and the
+// copies left exposed are short), then 512 MiB, so that a large call's copies overlap kernels
+uint32_t host_chunk_blocks(uint32_t block_log, uint32_t per_launch, uint32_t i) {
+  const size_t bytes = (size_t)(i == 0 ? 128 : 512) << 20;
+  return std::max<uint32_t>(1, std::min<uint32_t>(per_launch, (uint32_t)(bytes >> block_log)));
+}
+
 void plain_blocks(zc_ctx* c, uint64_t n, uint32_t B, uint32_t nb, uint64_t* d_off, uint32_t* d_len, cudaStream_t st) {
   if (!nb) return;
   c->stages.begin("k_plain_blocks", st);
@@ -267,14 +274,6 @@ int with_graph(zc_ctx* c, int kind, const uint64_t* key, int nkey, cudaStream_t 
   c->graph_cache.push_back(g);
   ZC_CUDA(cudaGraphLaunch(g.exec, st));
   return ZC_OK;
-}
-
-// host-pointer compress of nb blocks whose bytes lie in host memory [lo, lo + span)
-// blocks in chunk `i` of a host-pointer call: 128 MiB first (so the first kernels start early and the
-// copies left exposed are short), then 512 MiB, so that a large call's copies overlap kernels
-uint32_t host_chunk_blocks(uint32_t block_log, uint32_t per_launch, uint32_t i) {
-  const size_t bytes = (size_t)(i == 0 ? 128 : 512) << 20;
-  return std::max<uint32_t>(1, std::min<uint32_t>(per_launch, (uint32_t)(bytes >> block_log)));
 }
 
 // Compression of host-resident blocks in chunks through the two stages: chunk i's upload (copy stream)
@@ -428,7 +427,7 @@ void zc_close(zc_ctx* c) {
                     &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
                     &c->e_bits, &c->e_lanes, &c->e_freq, &c->e_lanelen, &c->e_sinfo, &c->e_slab, &c->d_lit, &c->d_tok,
                     &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta, &c->work,
-                    &c->a_desc, &c->a_work, &c->a_in, &c->a_out})
+                    &c->a_desc, &c->a_work})
     release(*b);
   if (c->h_meta.p) cudaFreeHost(c->h_meta.p);
   for (auto& S : c->pipe) {

@@ -272,19 +272,23 @@ void fill_pieces(std::vector<uint8_t>& h, const PieceDev& d, const Pieces& P) {
   put_section(h, d.part_len, P.part_len);
 }
 
-// k_crc_pieces + k_file_crcs over a solid stream on the device
-void launch_file_crcs(zc_ctx* c, const uint8_t* d_solid, const uint8_t* D, const PieceDev& d, const Pieces& P,
-                      const uint32_t* blk_crc, uint32_t* part_crc, uint8_t* table, uint32_t* entry_crc, cudaStream_t st) {
-  if (!P.part_off.empty()) {
-    zc::CrcArgs C{};
-    C.base = d_solid;
-    C.offs = reinterpret_cast<const uint64_t*>(D + d.part_off);
-    C.lens = reinterpret_cast<const uint32_t*>(D + d.part_len);
-    C.nb = (uint32_t)P.part_off.size();
-    C.crc = part_crc;
-    C.tables = c->d_crct;
-    zc::launch_crc(C, st, c->stages, "k_crc_pieces");
-  }
+// k_crc_pieces: the CRCs of np partial pieces (offsets from base, lengths: device arrays)
+void launch_piece_crcs(zc_ctx* c, const uint8_t* base, const uint64_t* offs, const uint32_t* lens, uint32_t np,
+                       uint32_t* part_crc, cudaStream_t st) {
+  if (!np) return;
+  zc::CrcArgs C{};
+  C.base = base;
+  C.offs = offs;
+  C.lens = lens;
+  C.nb = np;
+  C.crc = part_crc;
+  C.tables = c->d_crct;
+  zc::launch_crc(C, st, c->stages, "k_crc_pieces");
+}
+
+// k_file_crcs: every file's CRC from its pieces' (block and partial piece CRCs already computed)
+void launch_combine(zc_ctx* c, const uint8_t* D, const PieceDev& d, const Pieces& P, const uint32_t* blk_crc,
+                    const uint32_t* part_crc, uint8_t* table, uint32_t* entry_crc, cudaStream_t st) {
   const uint32_t nf = (uint32_t)P.entry.size();
   if (!nf) return;
   FileCrcArgs F{};
@@ -302,6 +306,14 @@ void launch_file_crcs(zc_ctx* c, const uint8_t* d_solid, const uint8_t* D, const
   c->stages.begin("k_file_crcs", st);
   k_file_crcs<<<(nf + 7) / 8, 256, 0, st>>>(F);
   c->stages.end(st);
+}
+
+// k_crc_pieces + k_file_crcs over a solid stream resident on the device
+void launch_file_crcs(zc_ctx* c, const uint8_t* d_solid, const uint8_t* D, const PieceDev& d, const Pieces& P,
+                      const uint32_t* blk_crc, uint32_t* part_crc, uint8_t* table, uint32_t* entry_crc, cudaStream_t st) {
+  launch_piece_crcs(c, d_solid, reinterpret_cast<const uint64_t*>(D + d.part_off),
+                    reinterpret_cast<const uint32_t*>(D + d.part_len), (uint32_t)P.part_off.size(), part_crc, st);
+  launch_combine(c, D, d, P, blk_crc, part_crc, table, entry_crc, st);
 }
 
 int write_device(zc_ctx* c, const uint8_t* d_solid, uint32_t bl, int level, const zc_entry* es, uint32_t ne,
@@ -463,6 +475,310 @@ int walk_blocks(const uint8_t* a, uint64_t len, const zc_archive_info& I, uint64
   return ZC_OK;
 }
 
+
+// the partial pieces that start in the stream range [lo, hi): indices [q0, q1) (pieces are in stream order)
+void pieces_in(const Pieces& P, uint64_t lo, uint64_t hi, uint32_t& q0, uint32_t& q1) {
+  q0 = (uint32_t)(std::lower_bound(P.part_off.begin(), P.part_off.end(), lo) - P.part_off.begin());
+  q1 = (uint32_t)(std::lower_bound(P.part_off.begin(), P.part_off.end(), hi) - P.part_off.begin());
+}
+
+void put_header(uint8_t* out, uint64_t n, uint64_t nb, uint32_t bl) {
+  memcpy(out, "ZERO", 4);
+  out[4] = 2;
+  out[5] = (uint8_t)bl;
+  out[6] = out[7] = 0;
+  for (int i = 0; i < 8; ++i) {
+    out[8 + i] = (uint8_t)(n >> (8 * i));
+    out[16 + i] = (uint8_t)(nb >> (8 * i));
+  }
+}
+
+// Host-pointer archive write.  The solid stream goes up in chunks of whole blocks (128 MiB, then 512 MiB)
+// through the context's two stages: a chunk's upload and the previous chunk's records coming down (copy
+// stream) overlap the chunk's kernels.  Each chunk's records are written from the start of its stage
+// buffer; the partial file pieces inside the chunk get their CRCs while it is resident.  At the end the
+// files' CRCs are combined on the device and the host writes the table and footer after the records.
+int write_host(zc_ctx* c, const uint8_t* solid, uint32_t bl, int level, zc_entry* es, uint32_t ne, uint8_t* out,
+               uint64_t out_cap, uint64_t* out_len) {
+  if (bad_block_log(bl)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  std::string why;
+  uint64_t n = 0;
+  if (!check_entries(es, ne, &n, why)) return fail(c, ZC_E_ARG, why);
+  if ((n && !solid) || !out) return fail(c, ZC_E_ARG, "no input or no output");
+  if (out_cap < kArchHdr) return fail(c, ZC_E_ARG, "the output buffer is too small");
+  const uint64_t B = 1ull << bl, nb64 = (n + B - 1) >> bl;
+  if (nb64 >= kPart) return fail(c, ZC_E_ARG, "too many blocks");
+  const uint32_t nb = (uint32_t)nb64;
+  Pieces P;
+  if (!cut_pieces(es, ne, bl, n, P, why)) return fail(c, ZC_E_ARG, why);
+  std::vector<uint8_t> table;
+  std::vector<uint32_t> pos;
+  build_table(es, ne, P, table, pos);
+  cudaStream_t st = c->stream, cs = c->cstream;
+  Layout L;
+  const PieceDev pd = place_pieces(L, P, false);
+  std::vector<uint8_t> h(L.at);
+  fill_pieces(h, pd, P);
+  const uint32_t nq = (uint32_t)P.part_off.size();
+  Layout W;
+  const size_t o_crc = W.put(4ull * nb), o_pcrc = W.put(4ull * nq), o_ecrc = W.put(4ull * ne), o_zero = W.put(8);
+  const size_t o_meth = W.put(nb), o_lens = W.put(4ull * nb), o_offs = W.put(8ull * nb);
+  ZC_CUDA(grow(c->a_desc, L.at));
+  ZC_CUDA(grow(c->a_work, W.at));
+  uint8_t* D = c->a_desc.as<uint8_t>();
+  uint8_t* X = c->a_work.as<uint8_t>();
+  ZC_CUDA(cudaMemcpyAsync(D, h.data(), L.at, cudaMemcpyHostToDevice, st));
+  ZC_CUDA(cudaMemsetAsync(X + o_zero, 0, 8, st));
+  uint32_t* d_crc = reinterpret_cast<uint32_t*>(X + o_crc);
+  uint32_t* d_pcrc = reinterpret_cast<uint32_t*>(X + o_pcrc);
+  put_header(out, n, nb64, bl);
+  uint64_t at = kArchHdr;
+  const uint32_t per_launch = enc_blocks_per_launch(bl);
+  struct Chunk {
+    uint32_t b0 = 0, k = 0;
+    size_t len_at = 0;  // where the chunk's records length lies in its stage's descriptors
+  };
+  Chunk prev;
+  bool have_prev = false;
+  // a finished chunk: its records length, then its records, come down on the copy stream
+  auto harvest = [&](zc_ctx::Stage& S, const Chunk& q) -> int {
+    ZC_CUDA(cudaStreamWaitEvent(cs, S.ev_done, 0));
+    uint64_t* h_len = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(S.h.p) + q.len_at);
+    ZC_CUDA(cudaMemcpyAsync(h_len, S.blk.as<uint8_t>() + q.len_at, 8, cudaMemcpyDeviceToHost, cs));
+    ZC_CUDA(cudaStreamSynchronize(cs));
+    const uint64_t rl = *h_len;
+    if (rl > out_cap - at) return fail(c, ZC_E_ARG, "the output buffer is too small");
+    if (rl) ZC_CUDA(cudaMemcpyAsync(out + at, S.out.p, rl, cudaMemcpyDeviceToHost, cs));
+    ZC_CUDA(cudaStreamSynchronize(cs));
+    at += rl;
+    return ZC_OK;
+  };
+  uint32_t it = 0;
+  for (uint32_t b0 = 0; b0 < nb; b0 += prev.k, ++it) {
+    zc_ctx::Stage& S = c->pipe[it & 1];
+    Chunk q;
+    q.b0 = b0;
+    q.k = std::min(host_chunk_blocks(bl, per_launch, it), nb - b0);
+    const uint32_t k = q.k;
+    const uint64_t lo = (uint64_t)b0 * B, span = std::min<uint64_t>(n - lo, (uint64_t)k * B);
+    uint32_t q0, q1;
+    pieces_in(P, lo, lo + span, q0, q1);
+    const uint32_t kq = q1 - q0;
+    // the stage's descriptors: block offsets and lengths (written by k_plain_blocks), the chunk's partial
+    // pieces (offsets from the chunk's start, lengths), the records length
+    Layout G;
+    const size_t g_off = G.put(8ull * k), g_len = G.put(4ull * k), g_poff = G.put(8ull * kq), g_plen = G.put(4ull * kq);
+    q.len_at = G.put(8);
+    ZC_CUDA(grow(S.in, span + 64));
+    ZC_CUDA(grow(S.out, (size_t)k * (B + zc::kRecHdr) + 64));
+    ZC_CUDA(grow(S.blk, G.at));
+    ZC_CUDA(grow_host(S.h, G.at));
+    uint8_t* hb = static_cast<uint8_t*>(S.h.p);
+    uint8_t* db = S.blk.as<uint8_t>();
+    uint64_t* hpo = reinterpret_cast<uint64_t*>(hb + g_poff);
+    uint32_t* hpl = reinterpret_cast<uint32_t*>(hb + g_plen);
+    for (uint32_t j = 0; j < kq; ++j) {
+      hpo[j] = P.part_off[q0 + j] - lo;
+      hpl[j] = P.part_len[q0 + j];
+    }
+    // upload on the copy stream (this stage's last chunk was harvested, so its buffers are free)
+    ZC_CUDA(cudaMemcpyAsync(S.in.p, solid + lo, span, cudaMemcpyHostToDevice, cs));
+    ZC_CUDA(cudaMemsetAsync(S.in.as<uint8_t>() + span, 0, 64, cs));
+    if (kq) ZC_CUDA(cudaMemcpyAsync(db + g_poff, hb + g_poff, q.len_at - g_poff, cudaMemcpyHostToDevice, cs));
+    ZC_CUDA(cudaEventRecord(S.ev_in, cs));
+    ZC_CUDA(cudaStreamWaitEvent(st, S.ev_in, 0));
+    uint64_t* ioff = reinterpret_cast<uint64_t*>(db + g_off);
+    uint32_t* ilen = reinterpret_cast<uint32_t*>(db + g_len);
+    plain_blocks(c, span, (uint32_t)B, k, ioff, ilen, st);
+    if (int r = encode_device(c, S.in.as<uint8_t>(), ioff, ilen, k, bl, level, X + o_meth + b0,
+                              reinterpret_cast<uint32_t*>(X + o_lens) + b0, d_crc + b0, S.out.as<uint8_t>(), S.out.n,
+                              reinterpret_cast<uint64_t*>(X + o_offs) + b0, reinterpret_cast<uint64_t*>(db + q.len_at),
+                              1, st, reinterpret_cast<const uint64_t*>(X + o_zero)))
+      return r;
+    launch_piece_crcs(c, S.in.as<uint8_t>(), reinterpret_cast<const uint64_t*>(db + g_poff),
+                      reinterpret_cast<const uint32_t*>(db + g_plen), kq, d_pcrc + q0, st);
+    ZC_CUDA(cudaEventRecord(S.ev_done, st));
+    if (have_prev)
+      if (int r = harvest(c->pipe[(it - 1) & 1], prev)) return r;
+    prev = q;
+    have_prev = true;
+  }
+  if (have_prev)
+    if (int r = harvest(c->pipe[(it - 1) & 1], prev)) return r;
+  // the files' CRCs, then the table and the footer
+  uint32_t* d_ecrc = reinterpret_cast<uint32_t*>(X + o_ecrc);
+  if (ne) ZC_CUDA(cudaMemsetAsync(d_ecrc, 0, 4ull * ne, st));
+  launch_combine(c, D, pd, P, d_crc, d_pcrc, nullptr, d_ecrc, st);
+  if (int r = check_launch(c, "archive launch")) return r;
+  std::vector<uint32_t> ec(ne);
+  if (ne) ZC_CUDA(cudaMemcpyAsync(ec.data(), d_ecrc, 4ull * ne, cudaMemcpyDeviceToHost, st));
+  ZC_CUDA(cudaStreamSynchronize(st));
+  for (size_t f = 0; f < P.entry.size(); ++f)
+    for (int b = 0; b < 4; ++b) table[pos[f] + b] = (uint8_t)(ec[P.entry[f]] >> (8 * b));
+  for (uint32_t i = 0; i < ne; ++i) es[i].crc = ec[i];
+  const uint64_t tl = table.size();
+  if (tl + kArchFoot > out_cap - at) return fail(c, ZC_E_ARG, "the output buffer is too small");
+  memcpy(out + at, table.data(), tl);
+  uint8_t* ft = out + at + tl;
+  const uint32_t tcrc = host_crc32(table.data(), tl);
+  for (int i = 0; i < 8; ++i) {
+    ft[i] = (uint8_t)(at >> (8 * i));
+    ft[8 + i] = (uint8_t)(tl >> (8 * i));
+  }
+  for (int i = 0; i < 4; ++i) ft[16 + i] = (uint8_t)(tcrc >> (8 * i));
+  memcpy(ft + 20, "ZEND", 4);
+  *out_len = at + tl + kArchFoot;
+  return ZC_OK;
+}
+
+// Host-pointer extract (out != NULL) or test.  The records go up in chunks of whole blocks through the
+// two stages: a chunk's upload and the previous chunk's raw bytes coming down overlap the chunk's decode.
+// Block CRCs and the partial file pieces' CRCs are computed while a chunk is resident; the files' CRCs
+// are combined on the device at the end.  Checks and messages in the reader's order (src/archive.h:
+// 611-634, 655-667): a damaged block, a block CRC, the stream's size, then each file's CRC.
+int extract_host(zc_ctx* c, const uint8_t* arch, uint64_t len, uint8_t* out, uint64_t out_cap) {
+  std::string why;
+  zc_archive_info I{};
+  std::vector<zc_entry> es;
+  if (parse_table(arch, len, &I, &es, why)) return fail(c, ZC_E_DATA, why);
+  if (I.n_blocks >= kPart) return fail(c, ZC_E_DATA, "archive damaged: block count");
+  // (the walk stops at the first damaged record, so n_blocks is bounded by the records' space first)
+  if (I.n_blocks > (I.table_off - kArchHdr) / zc::kRecHdr) return fail(c, ZC_E_DATA, "archive damaged: block header cut");
+  const uint32_t nb = (uint32_t)I.n_blocks, bl = I.block_log;
+  std::vector<uint64_t> coff(nb), ooff(nb);
+  std::vector<uint32_t> clen(nb), rlen(nb), rcrc(nb);
+  std::vector<uint8_t> meth(nb);
+  if (walk_blocks(arch, len, I, coff.data(), clen.data(), meth.data(), rlen.data(), rcrc.data(), why))
+    return fail(c, ZC_E_DATA, why);
+  if (out && out_cap < I.total_raw) return fail(c, ZC_E_ARG, "the output is smaller than the archive's stream");
+  uint64_t raw_sum = 0;
+  for (uint32_t b = 0; b < nb; ++b) {
+    ooff[b] = raw_sum;
+    raw_sum += rlen[b];
+  }
+  const bool sizes_agree = raw_sum == I.total_raw;
+  Pieces P;
+  if (sizes_agree && !cut_pieces(es.data(), (uint32_t)es.size(), bl, raw_sum, P, why)) return fail(c, ZC_E_DATA, why);
+  const uint32_t nq = (uint32_t)P.part_off.size(), ne = (uint32_t)es.size();
+  Layout L;
+  const PieceDev pd = place_pieces(L, P, false);
+  std::vector<uint8_t> h(L.at);
+  fill_pieces(h, pd, P);
+  Layout W;
+  const size_t o_crc = W.put(4ull * nb), o_err = W.put(4ull * nb), o_pcrc = W.put(4ull * nq), o_ecrc = W.put(4ull * ne);
+  cudaStream_t st = c->stream, cs = c->cstream;
+  ZC_CUDA(grow(c->a_desc, L.at));
+  ZC_CUDA(grow(c->a_work, W.at));
+  uint8_t* D = c->a_desc.as<uint8_t>();
+  uint8_t* X = c->a_work.as<uint8_t>();
+  ZC_CUDA(cudaMemcpyAsync(D, h.data(), L.at, cudaMemcpyHostToDevice, st));
+  uint32_t* d_crc = reinterpret_cast<uint32_t*>(X + o_crc);
+  uint32_t* d_err = reinterpret_cast<uint32_t*>(X + o_err);
+  uint32_t* d_pcrc = reinterpret_cast<uint32_t*>(X + o_pcrc);
+  const uint32_t per_launch = dec_blocks_per_launch(bl);
+  struct Chunk {
+    uint32_t b0 = 0, k = 0;
+    uint64_t raw_at = 0, raw_total = 0;
+  };
+  Chunk prev;
+  bool have_prev = false;
+  const bool copy_out = out && sizes_agree;  // (a stream of the wrong size is refused; nothing is written)
+  auto harvest = [&](zc_ctx::Stage& S, const Chunk& q) -> int {
+    ZC_CUDA(cudaStreamWaitEvent(cs, S.ev_done, 0));
+    if (copy_out && q.raw_total)
+      ZC_CUDA(cudaMemcpyAsync(out + q.raw_at, S.out.p, q.raw_total, cudaMemcpyDeviceToHost, cs));
+    ZC_CUDA(cudaStreamSynchronize(cs));
+    return ZC_OK;
+  };
+  uint32_t it = 0;
+  for (uint32_t b0 = 0; b0 < nb; b0 += prev.k, ++it) {
+    zc_ctx::Stage& S = c->pipe[it & 1];
+    Chunk q;
+    q.b0 = b0;
+    q.k = std::min(host_chunk_blocks(bl, per_launch, it), nb - b0);
+    const uint32_t k = q.k;
+    const uint64_t lo = coff[b0], hi = coff[b0 + k - 1] + clen[b0 + k - 1];
+    q.raw_at = ooff[b0];
+    q.raw_total = ooff[b0 + k - 1] + rlen[b0 + k - 1] - q.raw_at;
+    uint32_t q0 = 0, q1 = 0;
+    if (sizes_agree) pieces_in(P, q.raw_at, q.raw_at + q.raw_total, q0, q1);
+    const uint32_t kq = q1 - q0;
+    // the stage's descriptors: per block its body's offset in the chunk's span, its output offset in
+    // the chunk, lengths and method; the chunk's partial pieces (offsets in its output, lengths)
+    Layout G;
+    const size_t g_coff = G.put(8ull * k), g_ooff = G.put(8ull * k), g_clen = G.put(4ull * k), g_rlen = G.put(4ull * k);
+    const size_t g_meth = G.put(k), g_poff = G.put(8ull * kq), g_plen = G.put(4ull * kq);
+    ZC_CUDA(grow(S.in, (hi - lo) + 64));
+    ZC_CUDA(grow(S.out, q.raw_total + 64));
+    ZC_CUDA(grow(S.blk, G.at));
+    ZC_CUDA(grow_host(S.h, G.at));
+    uint8_t* hb = static_cast<uint8_t*>(S.h.p);
+    uint8_t* db = S.blk.as<uint8_t>();
+    for (uint32_t j = 0; j < k; ++j) {
+      reinterpret_cast<uint64_t*>(hb + g_coff)[j] = coff[b0 + j] - lo;
+      reinterpret_cast<uint64_t*>(hb + g_ooff)[j] = ooff[b0 + j] - q.raw_at;
+      reinterpret_cast<uint32_t*>(hb + g_clen)[j] = clen[b0 + j];
+      reinterpret_cast<uint32_t*>(hb + g_rlen)[j] = rlen[b0 + j];
+      hb[g_meth + j] = meth[b0 + j];
+    }
+    for (uint32_t j = 0; j < kq; ++j) {
+      reinterpret_cast<uint64_t*>(hb + g_poff)[j] = P.part_off[q0 + j] - q.raw_at;
+      reinterpret_cast<uint32_t*>(hb + g_plen)[j] = P.part_len[q0 + j];
+    }
+    if (hi > lo) ZC_CUDA(cudaMemcpyAsync(S.in.p, arch + lo, hi - lo, cudaMemcpyHostToDevice, cs));
+    ZC_CUDA(cudaMemsetAsync(S.in.as<uint8_t>() + (hi - lo), 0, 64, cs));
+    ZC_CUDA(cudaMemcpyAsync(db, hb, G.at, cudaMemcpyHostToDevice, cs));
+    ZC_CUDA(cudaEventRecord(S.ev_in, cs));
+    ZC_CUDA(cudaStreamWaitEvent(st, S.ev_in, 0));
+    if (int r = decode_device(c, S.in.as<uint8_t>(), reinterpret_cast<const uint64_t*>(db + g_coff),
+                              reinterpret_cast<const uint32_t*>(db + g_clen), db + g_meth,
+                              reinterpret_cast<const uint32_t*>(db + g_rlen), k, bl, S.out.as<uint8_t>(),
+                              reinterpret_cast<const uint64_t*>(db + g_ooff), d_crc + b0, d_err + b0, st))
+      return r;
+    launch_piece_crcs(c, S.out.as<uint8_t>(), reinterpret_cast<const uint64_t*>(db + g_poff),
+                      reinterpret_cast<const uint32_t*>(db + g_plen), kq, d_pcrc + q0, st);
+    ZC_CUDA(cudaEventRecord(S.ev_done, st));
+    if (have_prev)
+      if (int r = harvest(c->pipe[(it - 1) & 1], prev)) return r;
+    prev = q;
+    have_prev = true;
+  }
+  if (have_prev)
+    if (int r = harvest(c->pipe[(it - 1) & 1], prev)) return r;
+  uint32_t* d_ecrc = reinterpret_cast<uint32_t*>(X + o_ecrc);
+  if (ne) ZC_CUDA(cudaMemsetAsync(d_ecrc, 0, 4ull * ne, st));
+  if (sizes_agree) launch_combine(c, D, pd, P, d_crc, d_pcrc, nullptr, d_ecrc, st);
+  if (int r = check_launch(c, "archive launch")) return r;
+  std::vector<uint32_t> got(nb), err(nb), ecrc(ne);
+  if (nb) {
+    ZC_CUDA(cudaMemcpyAsync(got.data(), d_crc, 4ull * nb, cudaMemcpyDeviceToHost, st));
+    ZC_CUDA(cudaMemcpyAsync(err.data(), d_err, 4ull * nb, cudaMemcpyDeviceToHost, st));
+  }
+  if (ne) ZC_CUDA(cudaMemcpyAsync(ecrc.data(), d_ecrc, 4ull * ne, cudaMemcpyDeviceToHost, st));
+  ZC_CUDA(cudaStreamSynchronize(st));
+  char m[512];
+  for (uint32_t b = 0; b < nb; ++b) {
+    if (err[b]) {
+      snprintf(m, sizeof m, "block %u damaged (GPU decoder, code %u)", b, err[b]);
+      return fail(c, ZC_E_DATA, m);
+    }
+    if (got[b] != rcrc[b]) {
+      snprintf(m, sizeof m, "block %u does not match its checksum: the archive is damaged", b);
+      return fail(c, ZC_E_DATA, m);
+    }
+  }
+  if (!sizes_agree) {
+    snprintf(m, sizeof m, "archive damaged: the blocks hold %llu bytes, the table %llu", (unsigned long long)raw_sum,
+             (unsigned long long)I.total_raw);
+    return fail(c, ZC_E_DATA, m);
+  }
+  for (uint32_t i = 0; i < ne; ++i) {
+    if (es[i].is_dir || !es[i].size || ecrc[i] == es[i].crc) continue;
+    return fail(c, ZC_E_DATA, "file " + std::string(es[i].name, es[i].name_len) + " does not match its checksum");
+  }
+  return ZC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -488,40 +804,7 @@ int zc_archive_write(zc_ctx* c, const uint8_t* solid, uint32_t block_log, int le
                      uint32_t n_entries, uint8_t* out, uint64_t out_cap, uint64_t* out_len) {
   if (!c || !out_len) return ZC_E_ARG;
   ZC_CUDA(cudaSetDevice(c->device));
-  std::string why;
-  uint64_t n = 0;
-  if (!check_entries(entries, n_entries, &n, why)) return fail(c, ZC_E_ARG, why);
-  if (n && !solid) return fail(c, ZC_E_ARG, "no input");
-  const uint64_t bound = zc_archive_bound(entries, n_entries, block_log);
-  if (!bound) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
-  cudaStream_t st = c->stream;
-  ZC_CUDA(grow(c->a_in, n + 64));
-  const size_t ob = (bound + 255) & ~(size_t)255;
-  ZC_CUDA(grow(c->a_out, ob + 256 + 4ull * n_entries));
-  uint8_t* d_in = c->a_in.as<uint8_t>();
-  uint8_t* d_out = c->a_out.as<uint8_t>();
-  uint64_t* d_len = reinterpret_cast<uint64_t*>(d_out + ob);
-  uint32_t* d_ecrc = reinterpret_cast<uint32_t*>(d_out + ob + 256);
-  if (n) ZC_CUDA(cudaMemcpyAsync(d_in, solid, n, cudaMemcpyHostToDevice, st));
-  ZC_CUDA(cudaMemsetAsync(d_in + n, 0, 64, st));
-  if (int r = write_device(c, d_in, block_log, level, entries, n_entries, d_out, bound, d_len, d_ecrc, st)) return r;
-  uint64_t len = 0;
-  ZC_CUDA(cudaMemcpyAsync(&len, d_len, 8, cudaMemcpyDeviceToHost, st));
-  ZC_CUDA(cudaStreamSynchronize(st));
-  if (!len) return fail(c, ZC_E_DEVICE, "the archive did not fit its bound");
-  *out_len = len;
-  if (len > out_cap) {
-    char m[128];
-    snprintf(m, sizeof m, "the output buffer is too small: the archive has %llu bytes", (unsigned long long)len);
-    return fail(c, ZC_E_ARG, m);
-  }
-  if (!out) return fail(c, ZC_E_ARG, "no output");
-  std::vector<uint32_t> ec(n_entries);
-  ZC_CUDA(cudaMemcpyAsync(out, d_out, len, cudaMemcpyDeviceToHost, st));
-  if (n_entries) ZC_CUDA(cudaMemcpyAsync(ec.data(), d_ecrc, 4ull * n_entries, cudaMemcpyDeviceToHost, st));
-  ZC_CUDA(cudaStreamSynchronize(st));
-  for (uint32_t i = 0; i < n_entries; ++i) entries[i].crc = ec[i];
-  return ZC_OK;
+  return write_host(c, solid, block_log, level, entries, n_entries, out, out_cap, out_len);
 }
 
 int zc_archive_read_table(const uint8_t* arch, uint64_t len, zc_archive_info* info, zc_entry* entries, uint32_t cap,
@@ -550,104 +833,7 @@ int zc_archive_blocks(const uint8_t* arch, uint64_t len, const zc_archive_info* 
 int zc_archive_extract(zc_ctx* c, const uint8_t* arch, uint64_t len, uint8_t* out, uint64_t out_cap) {
   if (!c) return ZC_E_ARG;
   ZC_CUDA(cudaSetDevice(c->device));
-  std::string why;
-  zc_archive_info I{};
-  std::vector<zc_entry> es;
-  if (parse_table(arch, len, &I, &es, why)) return fail(c, ZC_E_DATA, why);
-  if (I.n_blocks >= kPart) return fail(c, ZC_E_DATA, "archive damaged: block count");
-  const uint32_t nb = (uint32_t)I.n_blocks, bl = I.block_log;
-  // the walk stops at the first damaged record, so n_blocks is bounded by the archive's length first
-  if (I.n_blocks > (I.table_off - kArchHdr) / zc::kRecHdr) return fail(c, ZC_E_DATA, "archive damaged: block header cut");
-  std::vector<uint64_t> coff(nb), ooff(nb);
-  std::vector<uint32_t> clen(nb), rlen(nb), rcrc(nb);
-  std::vector<uint8_t> meth(nb);
-  if (walk_blocks(arch, len, I, coff.data(), clen.data(), meth.data(), rlen.data(), rcrc.data(), why))
-    return fail(c, ZC_E_DATA, why);
-  if (out && out_cap < I.total_raw) return fail(c, ZC_E_ARG, "the output is smaller than the archive's stream");
-  uint64_t raw_sum = 0;
-  for (uint32_t b = 0; b < nb; ++b) {
-    coff[b] -= kArchHdr;
-    ooff[b] = raw_sum;
-    raw_sum += rlen[b];
-  }
-  const bool sizes_agree = raw_sum == I.total_raw;
-  Pieces P;
-  if (sizes_agree && !cut_pieces(es.data(), (uint32_t)es.size(), bl, raw_sum, P, why)) return fail(c, ZC_E_DATA, why);
-  // descriptors: per block, then the pieces
-  Layout L;
-  const size_t o_coff = L.put(8ull * nb), o_ooff = L.put(8ull * nb), o_clen = L.put(4ull * nb), o_rlen = L.put(4ull * nb);
-  const size_t o_meth = L.put(nb);
-  const PieceDev pd = place_pieces(L, P, false);
-  std::vector<uint8_t> h(L.at);
-  put_section(h, o_coff, coff);
-  put_section(h, o_ooff, ooff);
-  put_section(h, o_clen, clen);
-  put_section(h, o_rlen, rlen);
-  put_section(h, o_meth, meth);
-  fill_pieces(h, pd, P);
-  Layout W;
-  const size_t o_crc = W.put(4ull * nb), o_err = W.put(4ull * nb), o_pcrc = W.put(4 * P.part_off.size());
-  const size_t o_ecrc = W.put(4 * es.size());
-  const uint64_t span = I.table_off - kArchHdr;
-  cudaStream_t st = c->stream;
-  ZC_CUDA(grow(c->a_in, span + 64));
-  ZC_CUDA(grow(c->a_out, raw_sum + 64));
-  ZC_CUDA(grow(c->a_desc, L.at));
-  ZC_CUDA(grow(c->a_work, W.at));
-  uint8_t* d_in = c->a_in.as<uint8_t>();
-  uint8_t* d_solid = c->a_out.as<uint8_t>();
-  uint8_t* D = c->a_desc.as<uint8_t>();
-  uint8_t* X = c->a_work.as<uint8_t>();
-  if (span) ZC_CUDA(cudaMemcpyAsync(d_in, arch + kArchHdr, span, cudaMemcpyHostToDevice, st));
-  ZC_CUDA(cudaMemsetAsync(d_in + span, 0, 64, st));
-  ZC_CUDA(cudaMemcpyAsync(D, h.data(), L.at, cudaMemcpyHostToDevice, st));
-  uint32_t* d_crc = reinterpret_cast<uint32_t*>(X + o_crc);
-  uint32_t* d_err = reinterpret_cast<uint32_t*>(X + o_err);
-  const uint32_t per = dec_blocks_per_launch(bl);
-  for (uint32_t b0 = 0; b0 < nb; b0 += per) {
-    const uint32_t k = std::min(per, nb - b0);
-    if (int r = decode_device(c, d_in, reinterpret_cast<const uint64_t*>(D + o_coff) + b0,
-                              reinterpret_cast<const uint32_t*>(D + o_clen) + b0, D + o_meth + b0,
-                              reinterpret_cast<const uint32_t*>(D + o_rlen) + b0, k, bl, d_solid,
-                              reinterpret_cast<const uint64_t*>(D + o_ooff) + b0, d_crc + b0, d_err + b0, st))
-      return r;
-  }
-  uint32_t* d_ecrc = reinterpret_cast<uint32_t*>(X + o_ecrc);
-  if (!es.empty()) ZC_CUDA(cudaMemsetAsync(d_ecrc, 0, 4 * es.size(), st));
-  if (sizes_agree) launch_file_crcs(c, d_solid, D, pd, P, d_crc, reinterpret_cast<uint32_t*>(X + o_pcrc), nullptr, d_ecrc, st);
-  if (int r = check_launch(c, "archive launch")) return r;
-  std::vector<uint32_t> got(nb), err(nb), ecrc(es.size());
-  if (nb) {
-    ZC_CUDA(cudaMemcpyAsync(got.data(), d_crc, 4ull * nb, cudaMemcpyDeviceToHost, st));
-    ZC_CUDA(cudaMemcpyAsync(err.data(), d_err, 4ull * nb, cudaMemcpyDeviceToHost, st));
-  }
-  if (!es.empty()) ZC_CUDA(cudaMemcpyAsync(ecrc.data(), d_ecrc, 4 * es.size(), cudaMemcpyDeviceToHost, st));
-  ZC_CUDA(cudaStreamSynchronize(st));
-  char m[512];
-  for (uint32_t b = 0; b < nb; ++b) {
-    if (err[b]) {
-      snprintf(m, sizeof m, "block %u damaged (GPU decoder, code %u)", b, err[b]);
-      return fail(c, ZC_E_DATA, m);
-    }
-    if (got[b] != rcrc[b]) {
-      snprintf(m, sizeof m, "block %u does not match its checksum: the archive is damaged", b);
-      return fail(c, ZC_E_DATA, m);
-    }
-  }
-  if (!sizes_agree) {
-    snprintf(m, sizeof m, "archive damaged: the blocks hold %llu bytes, the table %llu", (unsigned long long)raw_sum,
-             (unsigned long long)I.total_raw);
-    return fail(c, ZC_E_DATA, m);
-  }
-  for (size_t i = 0; i < es.size(); ++i) {
-    if (es[i].is_dir || !es[i].size || ecrc[i] == es[i].crc) continue;
-    return fail(c, ZC_E_DATA, "file " + std::string(es[i].name, es[i].name_len) + " does not match its checksum");
-  }
-  if (out && raw_sum) {
-    ZC_CUDA(cudaMemcpyAsync(out, d_solid, raw_sum, cudaMemcpyDeviceToHost, st));
-    ZC_CUDA(cudaStreamSynchronize(st));
-  }
-  return ZC_OK;
+  return extract_host(c, arch, len, out, out_cap);
 }
 
 }  // extern "C"

@@ -96,9 +96,9 @@ struct zc_ctx {
   zch::DevBuf s_in, s_blk, s_out, s_meta;
   zch::HostBuf h_meta;
   zch::DevBuf work;  // the decoder fill's device work counter
-  // whole-archive calls: descriptors (entry table, file pieces), per-block results, and for the
-  // host-pointer forms the solid stream and the archive
-  zch::DevBuf a_desc, a_work, a_in, a_out;
+  // whole-archive calls: descriptors (entry table, file pieces) and per-block results (the host-pointer
+  // forms stream their data through the two stages below)
+  zch::DevBuf a_desc, a_work;
   // the host-pointer codec calls run in chunks through two stages: a chunk's copies (on cstream) overlap
   // the other chunk's kernels (on stream)
   struct Stage {
@@ -114,6 +114,9 @@ namespace zch {
 int fail(zc_ctx* c, int code, const std::string& msg);
 int cuda_fail(zc_ctx* c, cudaError_t e, const char* what);
 cudaError_t grow(DevBuf& b, size_t bytes);
+cudaError_t grow_host(HostBuf& b, size_t bytes);  // pinned
+// blocks in chunk `i` of a host-pointer call: 128 MiB first, then 512 MiB (at most per_launch)
+uint32_t host_chunk_blocks(uint32_t block_log, uint32_t per_launch, uint32_t i);
 bool bad_block_log(uint32_t bl);
 uint32_t enc_blocks_per_launch(uint32_t block_log);
 uint32_t dec_blocks_per_launch(uint32_t block_log);
