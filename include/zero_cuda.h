@@ -266,7 +266,9 @@ int zc_archive_write_device(zc_ctx *ctx, const uint8_t *d_solid, uint32_t block_
                             uint64_t *d_len, uint32_t *d_entry_crcs, void *stream);
 
 /* The same from host memory into host memory (synchronous): solid holds the files' bytes in entry order;
- * *out_len gets the archive's length and entries[i].crc each entry's CRC. */
+ * *out_len gets the archive's length and entries[i].crc each entry's CRC.  The stream goes through the GPU
+ * in chunks (128 MiB, then 512 MiB): a chunk's upload and the previous chunk's records coming down
+ * overlap the chunk's kernels.  out_cap = zc_archive_bound is always enough. */
 int zc_archive_write(zc_ctx *ctx, const uint8_t *solid, uint32_t block_log, int level, zc_entry *entries,
                      uint32_t n_entries, uint8_t *out, uint64_t out_cap, uint64_t *out_len);
 
@@ -291,7 +293,8 @@ int zc_archive_blocks(const uint8_t *arch, uint64_t len, const zc_archive_info *
  * archive held in host memory, as read_blocks + extract_archive / test_archive do (src/archive.h:566-635,
  * 747-785): every block decoded on the GPU, each block's CRC checked against its record, each file's
  * CRC (over its span of the solid stream) computed on the GPU and checked against the table.  ZC_E_DATA
- * for the first failing check, its message in zc_last_error. */
+ * for the first failing check, its message in zc_last_error.  The records go through the GPU in chunks
+ * that overlap their copies with the other chunk's decode, as zc_archive_write does. */
 int zc_archive_extract(zc_ctx *ctx, const uint8_t *arch, uint64_t len, uint8_t *out, uint64_t out_cap);
 
 /* Kernel launches this context has issued since it was opened (for accounting). */
