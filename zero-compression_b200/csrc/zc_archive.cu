@@ -514,6 +514,7 @@ int write_host(zc_ctx* c, const uint8_t* solid, uint32_t bl, int level, zc_entry
   std::vector<uint8_t> table;
   std::vector<uint32_t> pos;
   build_table(es, ne, P, table, pos);
+  if (table.size() >= 0xFFFFFFFFull) return fail(c, ZC_E_ARG, "the entry table is too large");
   cudaStream_t st = c->stream, cs = c->cstream;
   Layout L;
   const PieceDev pd = place_pieces(L, P, false);
