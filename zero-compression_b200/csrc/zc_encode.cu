@@ -864,6 +864,9 @@ __global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
   const uint32_t LC = lane_cap(A.B, s);
   uint8_t* end = A.lanes + (size_t)b * lanes_per_block(A.B) + lane_base(A.B, s) + (size_t)(k + 1) * LC;
   uint8_t* ptr = end;
+  // output bytes go down from the lane's (16-byte aligned) end; they are gathered four at a time, the
+  // first at bits 31..24, and stored as aligned words
+  uint32_t acc = 0, pend = 0;
   uint32_t x = kRansLow;
   // The stream in chunks of kRansChunk symbols (a whole number of rounds of the 64 lanes), last chunk
   // first: the CTA stages a chunk in shared memory with coalesced loads, then lane k codes its symbols
@@ -890,12 +893,22 @@ __global__ void __launch_bounds__(64) k_enc_rans(EncArgs A) {
         const uint32_t c = stage[t], e = fc[c], m = rcp[c];
         const uint32_t f = e & 0x1FFFu;
         const uint32_t xmax = f << (23 - kScaleBits + 8);
-        while (x >= xmax) { *--ptr = (uint8_t)x; x >>= 8; }
+        while (x >= xmax) {
+          acc |= (x & 0xFFu) << (24u - 8u * pend);
+          x >>= 8;
+          if (++pend == 4u) {
+            ptr -= 4;
+            *reinterpret_cast<uint32_t*>(ptr) = acc;
+            acc = 0;
+            pend = 0;
+          }
+        }
         const uint32_t q = f == 1 ? x : __umulhi(x, m) >> (e >> 25);
         x += ((e >> 13) & 0xFFFu) + q * (kScale - f);
       }
     }
   }
+  for (uint32_t i = 0; i < pend; ++i) *--ptr = (uint8_t)(acc >> (24u - 8u * i));  // the bytes still gathered
   ptr -= 4;
   st32(ptr, x);
   const uint32_t ll = (uint32_t)(end - ptr);

@@ -104,12 +104,12 @@ struct EncArgs {
 };
 
 // lane scratch layout per block: stream s starts at lane_base(s), each of its 64 lanes has lane_cap(s)
-// bytes (rANS emits at most 2 bytes per symbol plus a 4-byte flush)
+// bytes (rANS emits at most 2 bytes per symbol plus a 4-byte flush); every lane's end is 16-byte aligned
 __host__ __device__ inline uint32_t stream_cap(uint32_t B, uint32_t s) {
   return s == 0 ? B : s == 2 ? B / 5 + 64 : B / 4 + 16;
 }
-__host__ __device__ inline uint32_t lane_cap(uint32_t B, uint32_t s) {
-  return 2 * ((stream_cap(B, s) + 63) / 64) + 16;
+__host__ __device__ inline uint32_t lane_cap(uint32_t B, uint32_t s) {  // a multiple of 16: lanes end aligned
+  return (2 * ((stream_cap(B, s) + 63) / 64) + 16 + 15) & ~15u;
 }
 __host__ __device__ inline uint64_t lane_base(uint32_t B, uint32_t s) {
   uint64_t o = 0;
