@@ -196,3 +196,45 @@ def test_reader_never_reads_outside_the_buffer():
             Z.archive_blocks(bytes(b), info)
         except Z.DataError:
             pass
+
+
+def stored_archive(files, block_log):
+    """An archive written here with stored blocks only (the layout of src/archive.h:334-441):
+    files = [(name, bytes or None for a folder, mtime, attr)]."""
+    B = 1 << block_log
+    solid = b"".join(d for _, d, _, _ in files if d is not None)
+    nb = (len(solid) + B - 1) // B
+    out = [b"ZERO" + bytes([2, block_log, 0, 0]) + struct.pack("<QQ", len(solid), nb)]
+    for b in range(nb):
+        blk = solid[b * B:(b + 1) * B]
+        out.append(struct.pack("<IIB3xI", len(blk), len(blk), 0, zlib.crc32(blk)) + blk)
+    table = [struct.pack("<I", len(files))]
+    for name, data, mtime, attr in files:
+        nm = name.encode()
+        size = 0 if data is None else len(data)
+        crc = 0 if data is None else zlib.crc32(data)
+        table.append(struct.pack("<B3xI", 1 if data is None else 0, len(nm)) + nm + struct.pack("<QqII", size, mtime, attr, crc))
+    head = b"".join(out)
+    table = b"".join(table)
+    return head + table + struct.pack("<QQI", len(head), len(table), zlib.crc32(table)) + b"ZEND", solid
+
+
+def test_reader_fields_round_trip():
+    rng = np.random.default_rng(9)
+    files = [("dossier", None, 1700000000, 16),
+             ("dossier/été.txt", rng.integers(0, 256, 70000, dtype=np.uint8).tobytes(), -86400, 0x20),
+             ("dossier/sub", None, 0, 16),
+             ("dossier/sub/empty", b"", 5, 0),
+             ("dossier/sub/z", bytes(100), 2**40, 0xFFFFFFFF)]
+    a, solid = stored_archive(files, 16)
+    info, es = Z.read_table(a)
+    assert info["total_raw"] == len(solid) and info["n_blocks"] == 2 and info["n_entries"] == len(files)
+    for (name, data, mtime, attr), e in zip(files, es):
+        assert e.name == name and e.is_dir == (data is None) and e.mtime == mtime and e.attr == attr
+        assert e.size == (0 if data is None else len(data))
+        assert e.crc == (0 if data is None else zlib.crc32(data))
+    rec = Z.archive_blocks(a, info)
+    assert list(rec["methods"]) == [0, 0] and list(rec["raw_lens"]) == [65536, len(solid) - 65536]
+    got = b"".join(a[int(o):int(o) + int(n)] for o, n in zip(rec["offs"], rec["comp_lens"]))
+    assert got == solid
+    assert [int(c) for c in rec["crcs"]] == [zlib.crc32(solid[:65536]), zlib.crc32(solid[65536:])]
