@@ -8,6 +8,8 @@
 //   zero_dropin x <archive.zero> -o <folder>
 //   zero_dropin t <archive.zero>
 //   zero_dropin bench <file> [--block N] [--level L]     (in memory, as src/main.cpp:205-277 measures)
+//   zero_dropin c2 <file|folder>... -o <archive.zero> [--block N] [--level L]   (zc_archive_write)
+//   zero_dropin t2 <archive.zero>                                             (zc_archive_extract)
 #define ZERO_CUDA_DEFINE_GPU_ERROR
 #include "archive.h"  // reference: src/archive.h
 #include "zero_cuda_codec.hpp"
@@ -19,7 +21,7 @@
 namespace {
 
 int usage() {
-  fprintf(stderr, "usage: zero_dropin c|x|t|bench ...\n");
+  fprintf(stderr, "usage: zero_dropin c|x|t|bench|c2|t2 ...\n");
   return 2;
 }
 
@@ -59,6 +61,53 @@ int main(int argc, char** argv) {
       const zero::ExtractStats st = zero::test_archive(inputs.at(0), codec, rep);
       printf("%s: OK, %zu files, %llu bytes in %llu blocks\n", inputs.at(0).c_str(), st.files,
              (unsigned long long)st.raw, (unsigned long long)st.blocks);
+      return 0;
+    }
+    if (cmd == "c2" || cmd == "t2") {
+      // the container on the GPU (zc_archive_write / zc_archive_extract), as `zero c` / `zero t` would call
+      // it: the entries as the reference collects them (src/archive.h:170-250), the files read into one
+      // solid stream in entry order (a file that shrank while read gives zeros, src/archive.h:316-318)
+      zc_ctx* ctx = nullptr;
+      if (zc_open(&ctx, 0) != ZC_OK) {
+        const std::string m = ctx ? zc_last_error(ctx) : "zc_open failed";
+        zc_close(ctx);
+        throw std::runtime_error(m);
+      }
+      struct Closer { zc_ctx* c; ~Closer() { zc_close(c); } } closer{ctx};
+      if (cmd == "t2") {
+        std::ifstream f(inputs.at(0), std::ios::binary);
+        std::vector<uint8_t> arch((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+        if (zc_archive_extract(ctx, arch.data(), arch.size(), nullptr, 0) != ZC_OK) throw zb::Error(zc_last_error(ctx));
+        printf("%s: OK, every block and file checksum matches\n", inputs.at(0).c_str());
+        return 0;
+      }
+      const std::vector<zero::Entry> es = zero::collect(inputs, rep);
+      uint64_t total = 0;
+      for (const zero::Entry& e : es) total += e.dir ? 0 : e.size;
+      std::vector<uint8_t> solid(total + 1);
+      std::vector<zc_entry> ze(es.size());
+      size_t at = 0;
+      for (size_t i = 0; i < es.size(); ++i) {
+        const zero::Entry& e = es[i];
+        ze[i] = zc_entry{e.name.data(), (uint32_t)e.name.size(), e.dir ? 1u : 0u, e.size, e.mtime, e.attr, 0};
+        if (e.dir || !e.size) continue;
+        FILE* f = zero::open_file(e.source, "rb");
+        if (!f) throw zb::Error("cannot read " + e.name);
+        const size_t r = fread(solid.data() + at, 1, (size_t)e.size, f);
+        fclose(f);
+        if (r != e.size) memset(solid.data() + at + r, 0, (size_t)e.size - r);
+        at += (size_t)e.size;
+      }
+      std::vector<uint8_t> arch(zc_archive_bound(ze.data(), (uint32_t)ze.size(), block_log));
+      uint64_t len = 0;
+      if (arch.empty() || zc_archive_write(ctx, solid.data(), block_log, level, ze.data(), (uint32_t)ze.size(), arch.data(),
+                                           arch.size(), &len) != ZC_OK)
+        throw std::runtime_error(std::string("zc_archive_write: ") + zc_last_error(ctx));
+      FILE* o = fopen(out.c_str(), "wb");
+      if (!o || fwrite(arch.data(), 1, len, o) != len) throw zb::Error("writing " + out + " failed");
+      fclose(o);
+      printf("%s: %llu -> %llu bytes, the container written on the GPU\n", out.c_str(), (unsigned long long)total,
+             (unsigned long long)len);
       return 0;
     }
     if (cmd == "bench") {

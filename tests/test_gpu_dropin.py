@@ -124,3 +124,19 @@ def test_damaged_archive_is_refused(tree, tmp_path):
 def test_bench_entry_point(tree, tmp_path):
     r = run("bench", tree / "sub" / "b.bin", "--block", 18, "--level", 5)
     assert r.returncode == 0 and "identical" in r.stdout, r.stdout + r.stderr
+
+
+@need
+@pytest.mark.parametrize("block,level", [(16, 1), (18, 5), (20, 9)])
+def test_container_on_gpu_equals_compress_archive(tree, tmp_path, block, level):
+    """`zero c` with the whole container written on the GPU (zc_archive_write from C++, the entries as the
+    reference collects them): the file equals compress_archive's with the reference CPU codec, and
+    zc_archive_extract and the reference reader both check it."""
+    ours, ref = tmp_path / "c2.zero", tmp_path / "ref.zero"
+    r = run("c2", tree, "-o", ours, "--block", block, "--level", level)
+    assert r.returncode == 0, r.stderr
+    O.Ref.compress_archive([str(tree)], str(ref), block_log=block, level=level)
+    assert ours.read_bytes() == ref.read_bytes()
+    r = run("t2", ours)
+    assert r.returncode == 0 and "OK" in r.stdout, r.stderr
+    O.Ref.test_archive(str(ours))
