@@ -316,6 +316,18 @@ void launch_file_crcs(zc_ctx* c, const uint8_t* d_solid, const uint8_t* D, const
   launch_combine(c, D, d, P, blk_crc, part_crc, table, entry_crc, st);
 }
 
+// the archive header (src/archive.h:356-361): "ZERO", version 2, block_log, 0, total raw bytes, blocks
+void put_header(uint8_t* out, uint64_t n, uint64_t nb, uint32_t bl) {
+  memcpy(out, "ZERO", 4);
+  out[4] = 2;
+  out[5] = (uint8_t)bl;
+  out[6] = out[7] = 0;
+  for (int i = 0; i < 8; ++i) {
+    out[8 + i] = (uint8_t)(n >> (8 * i));
+    out[16 + i] = (uint8_t)(nb >> (8 * i));
+  }
+}
+
 int write_device(zc_ctx* c, const uint8_t* d_solid, uint32_t bl, int level, const zc_entry* es, uint32_t ne,
                  uint8_t* d_out, uint64_t out_cap, uint64_t* d_len, uint32_t* d_entry_crcs, cudaStream_t st) {
   if (bad_block_log(bl)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
@@ -357,13 +369,7 @@ int write_device(zc_ctx* c, const uint8_t* d_solid, uint32_t bl, int level, cons
   uint64_t* ends = reinterpret_cast<uint64_t*>(X + o_ends);
   uint32_t* crcs = reinterpret_cast<uint32_t*>(X + o_crcs);
   Head hd{};
-  memcpy(hd.b, "ZERO", 4);
-  hd.b[4] = 2;
-  hd.b[5] = (uint8_t)bl;
-  for (int i = 0; i < 8; ++i) {
-    hd.b[8 + i] = (uint8_t)(n >> (8 * i));
-    hd.b[16 + i] = (uint8_t)(nb64 >> (8 * i));
-  }
+  put_header(hd.b, n, nb64, bl);
   c->stages.begin("k_arch_head", st);
   k_arch_head<<<1, 32, 0, st>>>(hd, d_out, ends);
   c->stages.end(st);
@@ -480,17 +486,6 @@ int walk_blocks(const uint8_t* a, uint64_t len, const zc_archive_info& I, uint64
 void pieces_in(const Pieces& P, uint64_t lo, uint64_t hi, uint32_t& q0, uint32_t& q1) {
   q0 = (uint32_t)(std::lower_bound(P.part_off.begin(), P.part_off.end(), lo) - P.part_off.begin());
   q1 = (uint32_t)(std::lower_bound(P.part_off.begin(), P.part_off.end(), hi) - P.part_off.begin());
-}
-
-void put_header(uint8_t* out, uint64_t n, uint64_t nb, uint32_t bl) {
-  memcpy(out, "ZERO", 4);
-  out[4] = 2;
-  out[5] = (uint8_t)bl;
-  out[6] = out[7] = 0;
-  for (int i = 0; i < 8; ++i) {
-    out[8 + i] = (uint8_t)(n >> (8 * i));
-    out[16 + i] = (uint8_t)(nb >> (8 * i));
-  }
 }
 
 // Host-pointer archive write.  The solid stream goes up in chunks of whole blocks (128 MiB, then 512 MiB)
