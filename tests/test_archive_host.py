@@ -238,3 +238,37 @@ def test_reader_fields_round_trip():
     got = b"".join(a[int(o):int(o) + int(n)] for o, n in zip(rec["offs"], rec["comp_lens"]))
     assert got == solid
     assert [int(c) for c in rec["crcs"]] == [zlib.crc32(solid[:65536]), zlib.crc32(solid[65536:])]
+
+
+def test_reader_properties():
+    """Random entry lists (folders, empty and non-empty files, names of any UTF-8, any mtime and
+    attributes) at random block sizes: every field and block comes back as written; then random
+    corruptions of each archive end in a DataError or in a parse that stays inside the buffer."""
+    from hypothesis import given, settings, strategies as st, HealthCheck
+
+    entry = st.tuples(st.text(min_size=1, max_size=12), st.one_of(st.none(), st.binary(max_size=3000)),
+                      st.integers(-2**63, 2**63 - 1), st.integers(0, 2**32 - 1))
+
+    @settings(max_examples=60, deadline=None, suppress_health_check=list(HealthCheck))
+    @given(st.lists(entry, max_size=12), st.integers(16, 20), st.integers(0, 2**32 - 1))
+    def check(files, block_log, seed):
+        a, solid = stored_archive(files, block_log)
+        info, es = Z.read_table(a)
+        assert info["total_raw"] == len(solid) and info["n_entries"] == len(files)
+        for (name, data, mtime, attr), e in zip(files, es):
+            assert (e.name, e.is_dir, e.mtime, e.attr) == (name, data is None, mtime, attr)
+            assert e.size == (0 if data is None else len(data))
+        rec = Z.archive_blocks(a, info)
+        assert b"".join(a[int(o):int(o) + int(n)] for o, n in zip(rec["offs"], rec["comp_lens"])) == solid
+        rng = np.random.default_rng(seed)
+        for _ in range(8):
+            b = bytearray(a)
+            for _ in range(int(rng.integers(1, 4))):
+                b[int(rng.integers(0, len(b)))] = int(rng.integers(0, 256))
+            try:
+                i2, _ = Z.read_table(bytes(b))
+                Z.archive_blocks(bytes(b), i2)
+            except Z.DataError:
+                pass
+
+    check()
