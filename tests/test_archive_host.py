@@ -272,3 +272,42 @@ def test_reader_properties():
                 pass
 
     check()
+
+
+def test_collect_matches_the_reference(tmp_path):
+    """zero_cuda.collect gives the reference's entries, in its order: byte-sorted names in every folder
+    (upper case before lower case, '10' before '9', UTF-8 after ASCII), symlinks skipped, empty folders
+    and files kept, a repeated input kept once; read_solid gives the bytes the reference's blocks hold."""
+    if not O.Ref.available():
+        pytest.skip("oracle/_ref (built from the reference tree) is not present")
+    root = tmp_path / "data"
+    files = {"B.txt": b"upper", "a.txt": b"lower", "été.bin": bytes(range(256)) * 300, "z/deep/file": b"x" * 70000,
+             "z/empty": b"", "_": b"u", "10": b"ten", "9": b"nine"}
+    for rel, data in files.items():
+        p = root / rel
+        p.parent.mkdir(parents=True, exist_ok=True)
+        p.write_bytes(data)
+    (root / "emptydir").mkdir()
+    os.symlink("a.txt", root / "link")
+    single = tmp_path / "single.bin"
+    single.write_bytes(b"one file on its own" * 100)
+    for dp, dn, fn in os.walk(root):
+        for x in dn + fn:
+            os.utime(os.path.join(dp, x), (1700000000, 1700000000), follow_symlinks=False)
+    os.utime(root, (1700000000, 1700000000))
+    inputs = [str(root), str(single), str(root) + "/"]
+    ref = tmp_path / "r.zero"
+    O.Ref.compress_archive(inputs, str(ref), block_log=16, level=1)
+    a = ref.read_bytes()
+    info, es = Z.read_table(a)
+    got = Z.collect(inputs)
+    assert [(e.name, e.is_dir, e.size, e.mtime, e.attr) for e, _ in got] == \
+           [(e.name, e.is_dir, e.size, e.mtime, e.attr) for e in es]
+    rec = Z.archive_blocks(a, info)
+    out = bytearray()
+    for o, cl, m, rl in zip(rec["offs"], rec["comp_lens"], rec["methods"], rec["raw_lens"]):
+        body = a[int(o):int(o) + int(cl)]
+        out += body if m == 0 else O.Port.decompress_block(body, int(rl))
+    assert Z.read_solid(got) == bytes(out)
+    with pytest.raises(FileNotFoundError):
+        Z.collect([str(tmp_path / "missing")])

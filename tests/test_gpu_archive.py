@@ -219,3 +219,18 @@ def test_archive_over_several_encoder_launches(codec):
     torch.cuda.synchronize()
     assert int(d_len.item()) == len(got)
     assert d_out[:len(got)].cpu().numpy().tobytes() == got
+
+
+@need_ref
+@pytest.mark.parametrize("block,level", [(16, 9), (18, 5)])
+def test_archive_write_paths_equals_compress_archive(codec, tmp_path, block, level):
+    """`zero c` from Python: folders and files collected as the reference does, written on the GPU."""
+    root = tmp_path / "data"
+    make_tree(root, block)
+    single = tmp_path / "single.bin"
+    single.write_bytes(b"one file on its own" * 1000)
+    ref = tmp_path / "ref.zero"
+    O.Ref.compress_archive([str(root), str(single)], str(ref), block_log=block, level=level)
+    got, entries = codec.archive_write_paths([str(root), str(single)], block, level=level)
+    assert got == ref.read_bytes()
+    assert [e.crc for e in entries] == [e.crc for e in Z.read_table(got)[1]]

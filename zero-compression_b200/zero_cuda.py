@@ -158,6 +158,73 @@ def _c_entries(entries):
     return arr, keep
 
 
+def collect(inputs):
+    """The entries for a list of files and folders, collected as the reference's `zero c` does
+    (src/archive.h:167-250): a file is one entry under its own name; a folder is itself and everything in
+    it, under its name, sorted inside each folder by the UTF-8 bytes of the names; symbolic links are
+    skipped; a name already taken keeps its first entry.  Modification times are whole seconds.
+    Returns [(ArchiveEntry, source path)].  Raises FileNotFoundError for an input that does not exist."""
+    out, seen = [], set()
+
+    def add(e, src):
+        if e.name not in seen:
+            seen.add(e.name)
+            out.append((e, src))
+
+    def mtime(path):
+        try:
+            return int(os.stat(path).st_mtime)
+        except OSError:
+            return 0
+
+    def walk(folder, rel):
+        try:
+            names = os.listdir(folder)
+        except OSError:
+            return
+        for nm in sorted(names, key=os.fsencode):
+            path = os.path.join(folder, nm)
+            name = rel + "/" + nm
+            if os.path.islink(path):
+                continue
+            if os.path.isdir(path):
+                add(ArchiveEntry(name, 0, mtime(path), is_dir=True), path)
+                walk(path, name)
+            elif os.path.isfile(path):
+                try:
+                    size = os.path.getsize(path)
+                except OSError:
+                    size = 0
+                add(ArchiveEntry(name, size, mtime(path)), path)
+
+    for inp in inputs:
+        path = inp if os.path.isabs(inp) else os.path.join(os.getcwd(), inp)
+        while len(path) > 1 and path.endswith(os.sep):
+            path = path[:-1]
+        if not os.path.exists(path):
+            raise FileNotFoundError("not found: " + inp)
+        top = os.path.basename(path)
+        if os.path.isdir(path):
+            add(ArchiveEntry(top, 0, mtime(path), is_dir=True), path)
+            walk(path, top)
+        elif os.path.isfile(path):
+            add(ArchiveEntry(top, os.path.getsize(path), mtime(path)), path)
+    return out
+
+
+def read_solid(collected):
+    """The solid stream of collected entries: each file's bytes in entry order, exactly its recorded size
+    (a file that shrank since it was collected reads as zeros past its end, as src/archive.h:316-318)."""
+    parts = []
+    for e, src in collected:
+        if e.is_dir or not e.size:
+            continue
+        with open(src, "rb") as f:
+            data = f.read(e.size)
+        parts.append(data + bytes(e.size - len(data)))
+    return b"".join(parts)
+
+
 def archive_bound(entries, block_log):
     """The largest archive zc_archive_write can produce for these entries (0 for invalid ones)."""
     arr, _keep = _c_entries(entries)
@@ -444,6 +511,13 @@ class CudaCodec:
         for i, e in enumerate(entries):
             e.crc = int(arr[i].crc)
         return out[: n.value].tobytes()
+
+    def archive_write_paths(self, inputs, block_log, level=None):
+        """`zero c` for files and folders: the entries collected as the reference does, the files read in
+        entry order, the archive written on the GPU -> (archive bytes, entries with their CRCs)."""
+        got = collect(inputs)
+        entries = [e for e, _ in got]
+        return self.archive_write(read_solid(got), entries, block_log, level), entries
 
     def archive_write_device(self, d_solid, entries, block_log, d_out, d_len, d_entry_crcs=None, stream=0,
                              level=None, out_cap=None):
