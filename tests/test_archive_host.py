@@ -311,3 +311,46 @@ def test_collect_matches_the_reference(tmp_path):
     assert Z.read_solid(got) == bytes(out)
     with pytest.raises(FileNotFoundError):
         Z.collect([str(tmp_path / "missing")])
+
+
+def tree_state(root):
+    """Every path under root: (is folder, contents or None, modification time in seconds)."""
+    out = {}
+    for dp, dn, fn in os.walk(root):
+        for x in dn + fn:
+            p = os.path.join(dp, x)
+            data = None
+            if os.path.isfile(p):
+                with open(p, "rb") as f:
+                    data = f.read()
+            out[os.path.relpath(p, root)] = (os.path.isdir(p), data, os.stat(p).st_mtime_ns // 10**9)
+    return out
+
+
+def test_write_tree_matches_reference_extract(tmp_path):
+    """write_tree writes what the reference's extract_archive writes: the same files and folders, bytes
+    and modification times; an unsafe name is refused with the reference's message."""
+    if not O.Ref.available():
+        pytest.skip("oracle/_ref (built from the reference tree) is not present")
+    for ent in load_manifest()["archives"]:
+        a = golden(ent["name"])
+        info, es = Z.read_table(a)
+        rec = Z.archive_blocks(a, info)
+        solid = b"".join(a[int(o):int(o) + int(cl)] if m == 0 else O.Port.decompress_block(a[int(o):int(o) + int(cl)], int(rl))
+                         for o, cl, m, rl in zip(rec["offs"], rec["comp_lens"], rec["methods"], rec["raw_lens"]))
+        ours, ref = tmp_path / ("ours_" + ent["name"]), tmp_path / ("ref_" + ent["name"])
+        ours.mkdir()
+        Z.write_tree(es, solid, str(ours))
+        O.Ref.extract_archive(os.path.join(ARCH_DIR, ent["name"] + ".zero"), str(ref))
+        assert tree_state(ours) == tree_state(ref)
+    bad, solid = stored_archive([("ok", b"fine", 5, 0), ("../evil", b"no", 5, 0)], 16)
+    p = tmp_path / "bad.zero"
+    p.write_bytes(bad)
+    _, es = Z.read_table(bad)
+    out = tmp_path / "bad_ours"
+    out.mkdir()
+    with pytest.raises(Z.DataError, match="refused: unsafe name in the archive: ../evil"):
+        Z.write_tree(es, solid, str(out))
+    assert not (tmp_path / "evil").exists()
+    with pytest.raises(RuntimeError, match="refused: unsafe name in the archive: ../evil"):
+        O.Ref.extract_archive(str(p), str(tmp_path / "bad_ref"))

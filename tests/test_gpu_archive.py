@@ -234,3 +234,15 @@ def test_archive_write_paths_equals_compress_archive(codec, tmp_path, block, lev
     got, entries = codec.archive_write_paths([str(root), str(single)], block, level=level)
     assert got == ref.read_bytes()
     assert [e.crc for e in entries] == [e.crc for e in Z.read_table(got)[1]]
+
+
+@need_ref
+def test_archive_extract_to_equals_extract_archive(codec, tmp_path):
+    """`zero x` from Python: every CRC checked on the GPU, then the files written as extract_archive writes
+    them (the same files, folders, bytes and modification times)."""
+    from test_archive_host import tree_state
+    for ent in load_manifest()["archives"]:
+        ours, ref = tmp_path / ("ours_" + ent["name"]), tmp_path / ("ref_" + ent["name"])
+        codec.archive_extract_to(golden(ent["name"]), str(ours))
+        O.Ref.extract_archive(os.path.join(ARCH_DIR, ent["name"] + ".zero"), str(ref))
+        assert tree_state(ours) == tree_state(ref)

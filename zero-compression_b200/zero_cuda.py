@@ -225,6 +225,43 @@ def read_solid(collected):
     return b"".join(parts)
 
 
+def safe_name(name):
+    """A name from an archive is only ever written under the target folder (src/archive.h:511-523): not
+    empty, not absolute, no backslash or colon, and no empty, '.' or '..' component."""
+    if not name or name[0] == "/" or "\\" in name or ":" in name:
+        return False
+    return all(part not in ("", ".", "..") for part in name.split("/"))
+
+
+def write_tree(entries, solid, out_dir):
+    """Writes the solid stream back into files under out_dir as extract_archive does (src/archive.h:
+    640-745): entries in order, folders made as needed, each file its bytes of the stream, modification
+    times set (a zero time is left alone), folders' times last.  Raises DataError for an unsafe name or a
+    stream whose size is not the table's."""
+    _set = lambda path, t: t and os.utime(path, ns=(os.stat(path).st_atime_ns, t * 10**9))  # noqa: E731
+    mv = memoryview(solid)
+    pos = 0
+    for e in entries:
+        if not safe_name(e.name):
+            raise DataError("refused: unsafe name in the archive: " + e.name)
+        path = os.path.join(out_dir, *e.name.split("/"))
+        if e.is_dir:
+            os.makedirs(path, exist_ok=True)
+            continue
+        if pos + e.size > len(mv):
+            raise DataError("archive damaged: the table lists more data than the blocks hold")
+        os.makedirs(os.path.dirname(path) or out_dir, exist_ok=True)
+        with open(path, "wb") as f:
+            f.write(mv[pos:pos + e.size])
+        pos += e.size
+        _set(path, e.mtime)
+    if pos != len(mv):
+        raise DataError("archive damaged: more data than the table lists")
+    for e in entries:
+        if e.is_dir:
+            _set(os.path.join(out_dir, *e.name.split("/")), e.mtime)
+
+
 def archive_bound(entries, block_log):
     """The largest archive zc_archive_write can produce for these entries (0 for invalid ones)."""
     arr, _keep = _c_entries(entries)
@@ -518,6 +555,15 @@ class CudaCodec:
         got = collect(inputs)
         entries = [e for e, _ in got]
         return self.archive_write(read_solid(got), entries, block_log, level), entries
+
+    def archive_extract_to(self, arch, out_dir):
+        """`zero x`: every block and file checked on the GPU, then the files written under out_dir as the
+        reference's extract_archive writes them.  Returns the entries."""
+        solid = self.archive_extract(arch)
+        _, entries = read_table(arch)
+        os.makedirs(out_dir, exist_ok=True)
+        write_tree(entries, solid, out_dir)
+        return entries
 
     def archive_write_device(self, d_solid, entries, block_log, d_out, d_len, d_entry_crcs=None, stream=0,
                              level=None, out_cap=None):
