@@ -103,3 +103,78 @@ def test_two_ranks_assemble_the_single_rank_archive(tmp_path):
     whole = O.Port.crc32(raw[100000:500000].tobytes())
     assert shard.stream_crc([mt[2] for mt in metas], [mt[3] for mt in metas]) == whole
     assert shard.header(raw.size, nb, bl)[:6] == b"ZERO\x02\x10"
+
+
+def archive_rank_main(rank, world, port, root, out_dir):
+    """One rank of a whole-archive write: its block range coded, its records placed by the scan, its
+    piece of every file's CRC exchanged; rank 0 adds the header, the entry table and the footer."""
+    import torch.distributed as dist
+    import zero_cuda as Z
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    got = Z.collect([root])
+    entries = [e for e, _ in got]
+    raw = np.frombuffer(Z.read_solid(got), np.uint8)
+    bl = 16
+    B = 1 << bl
+    nb = (raw.size + B - 1) // B
+    b0, b1 = shard.block_range(nb, world, rank)
+    m, l, c, bodies = code_blocks(raw, b0, b1, bl, depth=O.depth_for_level(5))
+    recs = shard.records(raw[b0 * B:], m, l, c, bodies, bl)
+    off, total = shard.place(len(recs))
+    sizes = [0 if e.is_dir else e.size for e in entries]
+    mine = [(O.Port.crc32(raw[a:a + n].tobytes()) if n else 0, n)
+            for a, n in shard.file_pieces(sizes, b0 * B, min(b1 * B, raw.size))]
+    everyone = shard.gather_pieces(mine)
+    crcs = [shard.stream_crc([p[f][0] for p in everyone], [p[f][1] for p in everyone]) for f in range(len(entries))]
+    with open(os.path.join(out_dir, f"a{rank}.bin"), "wb") as f:
+        f.write(recs)
+    if rank == 0:
+        table = shard.entry_table(entries, crcs)
+        with open(os.path.join(out_dir, "head.bin"), "wb") as f:
+            f.write(shard.header(raw.size, nb, bl))
+        with open(os.path.join(out_dir, "tail.bin"), "wb") as f:
+            f.write(table + shard.footer(24 + total, table))
+    with open(os.path.join(out_dir, f"a{rank}.off"), "w") as f:
+        f.write(str(off))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_ranks_write_the_reference_archive(tmp_path):
+    """Two gloo ranks write one whole archive of a folder (files straddling the ranks' block ranges):
+    the bytes equal the reference's compress_archive of the same folder."""
+    import datagen as G
+    if not O.Ref.available():
+        import pytest
+        pytest.skip("oracle/_ref (built from the reference tree) is not present")
+    root = tmp_path / "data"
+    files = {"a.txt": G.text_mix(200000, 3).tobytes(), "m/b.lz": G.lz_mix(300000, 16, 4).tobytes(),
+             "m/empty": b"", "m/z.rnd": G.random_bytes(70000, 5).tobytes(), "q": b"tiny"}
+    for rel, data in files.items():
+        p = root / rel
+        p.parent.mkdir(parents=True, exist_ok=True)
+        p.write_bytes(data)
+    (root / "n").mkdir()
+    for dp, dn, fn in os.walk(root):
+        for x in dn + fn:
+            os.utime(os.path.join(dp, x), (1700000000, 1700000000))
+    os.utime(root, (1700000000, 1700000000))
+    world = 2
+    port = free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=archive_rank_main, args=(r, world, port, str(root), str(tmp_path))) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    parts = [(tmp_path / "head.bin").read_bytes()]
+    for r in range(world):
+        assert int((tmp_path / f"a{r}.off").read_text()) == sum(len(x) for x in parts) - 24
+        parts.append((tmp_path / f"a{r}.bin").read_bytes())
+    parts.append((tmp_path / "tail.bin").read_bytes())
+    ref = tmp_path / "ref.zero"
+    O.Ref.compress_archive([str(root)], str(ref), block_log=16, level=5)
+    assert b"".join(parts) == ref.read_bytes()

@@ -5,7 +5,8 @@ of the solid stream's blocks with no data exchange.  Writing one archive needs a
 rank's total record bytes (16-byte block record + body, src/archive.h:389-403), scanned across ranks to
 give each rank the offset of its first record.  CRCs of files that straddle two ranks' ranges combine
 with crc32::combine (src/crc32.h:60-66).  The exchange is one all-gather of one 64-bit value per rank
-(torch.distributed: NCCL between GPUs, gloo on the CPU).
+(torch.distributed: NCCL between GPUs, gloo on the CPU), and, for the entry table, one all-gather of each
+rank's (crc, length) piece of every file.
 """
 import struct
 
@@ -63,6 +64,44 @@ def stream_crc(part_crcs, part_lens):
     for c, n in zip(part_crcs, part_lens):
         crc = crc_combine(crc, c, n)
     return crc
+
+
+def file_pieces(sizes, lo, hi):
+    """For files of `sizes` laid end to end in the solid stream (folders have size 0): each file's part
+    inside the stream range [lo, hi) as (offset in the stream, length); (0, 0) for a file outside it."""
+    out, at = [], 0
+    for n in sizes:
+        a, b = max(at, lo), min(at + n, hi)
+        out.append((a, b - a) if b > a else (0, 0))
+        at += n
+    return out
+
+
+def gather_pieces(pieces, group=None):
+    """All ranks: every rank's per-file (crc, length) pieces, in rank order (one all-gather of objects)."""
+    import torch.distributed as dist
+    if group is None and not (dist.is_available() and dist.is_initialized()):
+        return [pieces]
+    out = [None] * dist.get_world_size(group)
+    dist.all_gather_object(out, pieces, group=group)
+    return out
+
+
+def entry_table(entries, crcs):
+    """The entry table (src/archive.h:416-429): u32 count; per entry u8 type (1 = folder), 3 zero bytes,
+    u32 name length, the name, u64 size, u64 mtime, u32 attributes, u32 CRC."""
+    out = bytearray(struct.pack("<I", len(entries)))
+    for e, crc in zip(entries, crcs):
+        nm = e.name.encode("utf-8", "surrogateescape")
+        out += struct.pack("<B3xI", 1 if e.is_dir else 0, len(nm)) + nm
+        out += struct.pack("<QqII", e.size, e.mtime, e.attr, crc & 0xFFFFFFFF)
+    return bytes(out)
+
+
+def footer(table_off, table):
+    """The footer (src/archive.h:430-435): u64 table offset, u64 table length, u32 CRC of the table, "ZEND"."""
+    import zlib
+    return struct.pack("<QQI", table_off, len(table), zlib.crc32(table)) + b"ZEND"
 
 
 def header(total_raw, n_blocks, block_log):
