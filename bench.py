@@ -164,7 +164,10 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded lz_mix generator)",
-        "config": workload_config(args),
+        "config": dict(workload_config(args), sample_bytes=sample,
+                       workload=f"lz_mix {args.size_mib} MiB per GPU (each step times a {sample >> 20} MiB sample of "
+                                f"it on the host cores), block {args.block} ({B >> 10} KiB), level {args.level}: "
+                                f"compress then extract (bit-exact round trip)"),
         "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": cores, "kind": kind, "sample": desc},
         "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -112,16 +112,18 @@ int zc_decompress_device(zc_ctx *ctx, const uint8_t *d_comp, const uint64_t *d_c
  * that cannot call cudaMalloc -- a plugin in a host process that budgets all device memory itself (an
  * admission-controlled server, a framework that owns its allocator), or a latency-bound path where
  * cudaMalloc / cudaFree would synchronise the device and stall other streams.  Arguments and results are
- * those of zc_decompress_device (all device pointers, work queued on `stream`), without a context.
- * Scratch is one fixed __device__ array of ZC_NOALLOC_SCRATCH_BYTES inside the library, held by every GPU
- * that loads the library until the process exits.  A block of 2^b bytes needs 2^b + 3*(2^b/4 + 16) +
- * (2^b/5 + 64) bytes of it (each part rounded up to 256, plus 256): at most 64 blocks of 64 KiB, 16 of
- * 256 KiB or 4 of 1 MiB per call; more returns ZC_E_ARG and touches nothing.
- * The first call on a device sets that device up (it looks up the arrays' device addresses and fills the
- * CRC tables, with the device current); make that first call before any stream capture.  Every call on a
- * device shares the one scratch array, so calls whose work overlaps on the GPU race: keep them on one
- * stream, or order them.  d_err is cleared by the call itself. */
-#define ZC_NOALLOC_SCRATCH_BYTES ((size_t)8 << 20)
+ * those of zc_decompress_device (all device pointers, work queued on `stream`), without a context; it runs
+ * the same decoder kernels.  Scratch is one fixed __device__ array of ZC_NOALLOC_SCRATCH_BYTES inside the
+ * library, held by every GPU that loads the library until the process exits.  A call of nb blocks of B =
+ * 2^b bytes needs 256 + nb*B + 3*nb*(B/4 + 16) + nb*(B/5 + 64) + 76*nb + 16*nb*(B/4 + 16) bytes of it
+ * (each of those nine parts rounded up to a multiple of 256): at most 42 blocks of 64 KiB, 21 of 128 KiB,
+ * 10 of 256 KiB, 5 of 512 KiB or 2 of 1 MiB per call; more returns ZC_E_ARG and touches nothing.
+ * The first call on a device sets that device up: with the device current it looks up the array's device
+ * address (and again whenever the device's context has changed, as after cudaDeviceReset); make that
+ * first call before any stream capture.  Every call on a device shares the one scratch array, so calls
+ * whose work overlaps on the GPU race: keep them on one stream, or order them.  d_err is cleared by the
+ * call itself, and so is the one scratch word that must start at zero. */
+#define ZC_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 int zc_decompress_noalloc(const uint8_t *d_comp, const uint64_t *d_comp_offs, const uint32_t *d_comp_lens,
                           const uint8_t *d_methods, const uint32_t *d_raw_lens, uint32_t nb, uint32_t block_log,
                           uint8_t *d_out, const uint64_t *d_out_offs, uint32_t *d_crcs, uint32_t *d_err, void *stream);

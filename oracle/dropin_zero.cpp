@@ -10,9 +10,16 @@
 //   zero_dropin bench <file> [--block N] [--level L]     (in memory, as src/main.cpp:205-277 measures)
 //   zero_dropin c2 <file|folder>... -o <archive.zero> [--block N] [--level L]   (zc_archive_write)
 //   zero_dropin t2 <archive.zero>                                             (zc_archive_extract)
+//
+// --safe puts zero::SafeCudaCodec (include/zero_cuda_safe.hpp) in place of the plain CudaCodec, as the
+// reference's choose_codec puts SafeCodec around its GpuCodec; --batch-kib N caps its batches (so that a
+// small job has several, and a failure injected with ZC_FAIL_AFTER=n can fall in the middle of a job).
 #define ZERO_CUDA_DEFINE_GPU_ERROR
 #include "archive.h"  // reference: src/archive.h
 #include "zero_cuda_codec.hpp"
+#include "zero_cuda_safe.hpp"
+
+#include <memory>
 
 #include <cstdio>
 #include <fstream>
@@ -34,17 +41,29 @@ int main(int argc, char** argv) {
   std::string out;
   uint32_t block_log = 18;
   int level = 5;
+  bool safe = false;
+  size_t batch_kib = 0;
   for (int i = 2; i < argc; ++i) {
     const std::string s = argv[i];
     if (s == "-o" && i + 1 < argc) out = argv[++i];
+    else if (s == "--safe") safe = true;
+    else if (s == "--batch-kib" && i + 1 < argc) batch_kib = (size_t)atoll(argv[++i]);
     else if (s == "--block" && i + 1 < argc) block_log = (uint32_t)atoi(argv[++i]);
     else if (s == "--level" && i + 1 < argc) level = atoi(argv[++i]);
     else inputs.push_back(s);
   }
   try {
-    zero::CudaCodec codec(level);
     zero::Report rep;
     rep.log = [](const std::string& m) { fprintf(stderr, "%s\n", m.c_str()); };
+    std::unique_ptr<zero::Codec> owned;
+    if (safe) {
+      auto sc = std::make_unique<zero::SafeCudaCodec>(level, 0, &rep);
+      sc->batch_cap = batch_kib << 10;
+      owned = std::move(sc);
+    } else {
+      owned = std::make_unique<zero::CudaCodec>(level);
+    }
+    zero::Codec& codec = *owned;
     if (cmd == "c") {
       const zero::CompressStats st = zero::compress_archive(inputs, out, codec, block_log, rep);
       printf("%s: %llu -> %llu bytes, %llu blocks (%llu stored), codec %.3f s\n", out.c_str(),

@@ -140,3 +140,61 @@ def test_container_on_gpu_equals_compress_archive(tree, tmp_path, block, level):
     r = run("t2", ours)
     assert r.returncode == 0 and "OK" in r.stdout, r.stderr
     O.Ref.test_archive(str(ours))
+
+
+def run_env(env, *args):
+    return subprocess.run([DROPIN] + [str(a) for a in args], capture_output=True, text=True, timeout=600,
+                          env=dict(os.environ, **env))
+
+
+@need
+@pytest.mark.parametrize("fail_after", [0, 3])
+def test_safe_codec_finishes_the_job_after_a_device_failure(tree, tmp_path, fail_after):
+    """SafeCudaCodec, the reference's SafeCodec contract (src/safe_codec.h:10-50) over the B200 codec.
+    ZC_FAIL_AFTER=n makes the context's (n+1)-th codec call fail with ZC_E_DEVICE before it launches
+    anything: that batch and every later one go to the reference's CPU codec, the report says so once,
+    and the archive is still the one compress_archive writes; extraction across the same failure (the
+    first batch, or one in the middle of the job) is bit-exact."""
+    ours, ref = tmp_path / "safe.zero", tmp_path / "ref.zero"
+    env = {"ZC_FAIL_AFTER": str(fail_after)}
+    r = run_env(env, "c", tree, "-o", ours, "--block", 16, "--level", 5, "--safe", "--batch-kib", 256)
+    assert r.returncode == 0, r.stderr
+    assert r.stderr.count("GPU stopped working") == 1 and "ZC_FAIL_AFTER" in r.stderr, r.stderr
+    O.Ref.compress_archive([str(tree)], str(ref), block_log=16, level=5)
+    assert ours.read_bytes() == ref.read_bytes()
+    out = tmp_path / "x"
+    r = run_env(env, "x", ours, "-o", out, "--safe", "--batch-kib", 256)
+    assert r.returncode == 0, r.stderr
+    assert r.stderr.count("GPU stopped working") == 1, r.stderr
+    assert tree_digest(out / "data") == tree_digest(tree)
+
+
+@need
+def test_safe_codec_without_failure_stays_on_the_gpu(tree, tmp_path):
+    ours, ref = tmp_path / "safe.zero", tmp_path / "ref.zero"
+    r = run_env({}, "c", tree, "-o", ours, "--block", 18, "--level", 9, "--safe", "--batch-kib", 512)
+    assert r.returncode == 0 and "GPU" not in r.stderr, r.stderr
+    O.Ref.compress_archive([str(tree)], str(ref), block_log=18, level=9)
+    assert ours.read_bytes() == ref.read_bytes()
+    r = run_env({}, "t", ours, "--safe")
+    assert r.returncode == 0 and "OK" in r.stdout and "GPU" not in r.stderr, r.stderr
+
+
+@need
+def test_safe_codec_damaged_block_is_redone_on_the_cpu(tree, tmp_path):
+    """A damaged payload is a data error, not a device failure: the GPU refuses the batch (ZC_E_DATA), the
+    CPU codec decodes it again and reports the damage with the reference's own message, and the GPU is not
+    given up."""
+    good = tmp_path / "good.zero"
+    O.Ref.compress_archive([str(tree)], str(good), block_log=16, level=5)
+    data = bytearray(good.read_bytes())
+    assert data[24 + 8] == 1  # block 0 is ZB2-coded (its record's method byte)
+    data[24 + 16:24 + 20] = b"\xff\xff\xff\x7f"  # its token count: far above what the block can hold
+    bad = tmp_path / "bad.zero"
+    bad.write_bytes(bytes(data))
+    with pytest.raises(RuntimeError) as cpu_err:
+        O.Ref.test_archive(str(bad))
+    r = run_env({}, "t", bad, "--safe")
+    assert r.returncode != 0
+    assert str(cpu_err.value) in r.stderr, (str(cpu_err.value), r.stderr)
+    assert "GPU stopped working" not in r.stderr

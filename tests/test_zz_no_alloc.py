@@ -11,13 +11,23 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 ZC_E_ARG = 4
-SCRATCH = 8 << 20
+SCRATCH = 16 << 20
+META_BYTES = 76  # per block: the framing record
 
 
-def per_block(block_log):
+def need(nb, block_log):
+    """Scratch bytes a call of nb blocks takes (the formula of include/zero_cuda.h)."""
     up = lambda x: (x + 255) & ~255
     B = 1 << block_log
-    return up(B) + 3 * up(B // 4 + 16) + up(B // 5 + 64) + 256
+    TC, EC = B // 4 + 16, B // 5 + 64
+    return 256 + up(nb * B) + 3 * up(nb * TC) + up(nb * EC) + up(nb * META_BYTES) + 4 * up(nb * TC * 4)
+
+
+def limit(block_log):
+    nb = 0
+    while need(nb + 1, block_log) <= SCRATCH:
+        nb += 1
+    return nb
 
 
 @pytest.fixture(scope="module")
@@ -87,7 +97,7 @@ def test_noalloc_matches_device_entry_point_twice(env):
     ]
     for data in inputs:  # two calls in a row, different inputs: the shared scratch keeps the last call's bytes
         blk = make_blocks(torch, codec, data, block_log)
-        assert blk["nb"] * per_block(block_log) <= SCRATCH
+        assert need(blk["nb"], block_log) <= SCRATCH
         (o1, c1, e1), (o2, c2, e2) = decode_both(torch, lib, codec, blk, block_log)
         assert o2 == o1 == data
         assert np.array_equal(c2, c1) and np.array_equal(e2, e1) and not e1.any()
@@ -106,10 +116,25 @@ def test_noalloc_damaged_block_status_matches(env):
     assert np.array_equal(c2[good], c1[good])
 
 
-def test_noalloc_rejects_beyond_scratch(env):
+def test_noalloc_limits_are_the_documented_ones():
+    assert [limit(bl) for bl in (16, 17, 18, 19, 20)] == [42, 21, 10, 5, 2]
+
+
+@pytest.mark.parametrize("block_log", [16, 18, 20])
+def test_noalloc_exactly_at_the_limit(env, block_log):
+    """nb = the limit decodes; nb = the limit + 1 is refused before anything runs."""
     torch, lib, codec = env
-    block_log = 20
-    nb = SCRATCH // per_block(block_log) + 1
+    import datagen as G
+    nb = limit(block_log)
+    data = G.lz_mix(nb << block_log, block_log, 50 + block_log).tobytes()
+    blk = make_blocks(torch, codec, data, block_log)
+    assert blk["nb"] == nb
+    (o1, c1, e1), (o2, c2, e2) = decode_both(torch, lib, codec, blk, block_log)
+    assert o2 == o1 == data and np.array_equal(c2, c1) and not e2.any()
+    check_refused(torch, lib, block_log, nb + 1)
+
+
+def check_refused(torch, lib, block_log, nb):
     dev = torch.device("cuda", 0)
     z64 = torch.zeros(nb, dtype=torch.int64, device=dev)
     z32 = torch.zeros(nb, dtype=torch.int32, device=dev)

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -139,7 +140,7 @@ int ensure_dec(zc_ctx* c, uint32_t nb, uint32_t block_log) {
       {&c->d_lit, (size_t)nb * B}, {&c->d_tok, (size_t)nb * TC}, {&c->d_sym, (size_t)nb * TC},
       {&c->d_grp, (size_t)nb * TC}, {&c->d_ext, (size_t)nb * EC}, {&c->d_meta, (size_t)nb * sizeof(zc::DecMeta)},
       {&c->d_tks, (size_t)nb * TC * 4}, {&c->d_tkm, (size_t)nb * TC * 4}, {&c->d_tkd, (size_t)nb * TC * 4},
-      {&c->d_tkl, (size_t)nb * TC * 4}, {&c->d_tot, (size_t)nb * 8}};
+      {&c->d_tkl, (size_t)nb * TC * 4}};
   return ensure(c, need);
 }
 
@@ -154,6 +155,19 @@ uint32_t enc_blocks_per_launch(uint32_t block_log) {
 // every SM busy; about 6 bytes of scratch per output byte)
 uint32_t dec_blocks_per_launch(uint32_t block_log) {
   return (uint32_t)std::min<size_t>(((size_t)4 << 30) >> block_log, 1u << 20);
+}
+
+// The test injector (src/safe_codec.h:17 has the reference's): with ZC_FAIL_AFTER=n in the environment
+// when the context was opened, the (n+1)-th codec call on it fails with ZC_E_DEVICE before it launches
+// anything, and so does every later call: a lost device stays lost.  Without it, nothing happens.
+int gate(zc_ctx* c) {
+  if (c->lost) return fail(c, ZC_E_DEVICE, "the GPU was lost earlier (device failure injected by ZC_FAIL_AFTER)");
+  if (c->fail_after == 0) {
+    c->lost = true;
+    return fail(c, ZC_E_DEVICE, "device failure injected by ZC_FAIL_AFTER");
+  }
+  if (c->fail_after > 0) --c->fail_after;
+  return ZC_OK;
 }
 
 int check_launch(zc_ctx* c, const char* what) {
@@ -209,7 +223,7 @@ int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs,
   A.s_lit = c->d_lit.as<uint8_t>(); A.s_tok = c->d_tok.as<uint8_t>(); A.s_sym = c->d_sym.as<uint8_t>();
   A.s_grp = c->d_grp.as<uint8_t>(); A.s_ext = c->d_ext.as<uint8_t>(); A.meta = c->d_meta.as<zc::DecMeta>();
   A.tk_start = c->d_tks.as<uint32_t>(); A.tk_ms = c->d_tkm.as<uint32_t>(); A.tk_d = c->d_tkd.as<uint32_t>();
-  A.tk_lik = c->d_tkl.as<uint32_t>(); A.tot_op = c->d_tot.as<uint32_t>(); A.tot_li = A.tot_op + nb;
+  A.tk_lik = c->d_tkl.as<uint32_t>();
   const Shape& sh = c->shape[block_log - zc::kMinBlockLog][level_class(c->level)];
   A.ring_log = sh.ring_log; A.fill_warps = sh.fill_warps;
   A.work = c->work.as<uint32_t>() + 1;
@@ -387,6 +401,7 @@ int zc_open(zc_ctx** out, int device) {
   zc_ctx* c = new zc_ctx;
   c->device = device;
   c->stages.impl = &c->records;
+  if (const char* fa = getenv("ZC_FAIL_AFTER")) c->fail_after = atoll(fa);
   cudaError_t e = cudaSetDevice(device);
   cudaDeviceProp prop;
   if (e == cudaSuccess) e = cudaGetDeviceProperties(&prop, device);
@@ -426,7 +441,7 @@ void zc_close(zc_ctx* c) {
   for (DevBuf* b : {&c->e_tmp_pos, &c->e_srt_pos, &c->e_minfo, &c->e_scnt, &c->e_tk_seg, &c->e_tmp_h, &c->e_srt_h, &c->e_tk_i,
                     &c->e_tk_m, &c->e_tk_d, &c->e_bcnt, &c->e_lit, &c->e_tok, &c->e_ext, &c->e_sym, &c->e_grp,
                     &c->e_bits, &c->e_lanes, &c->e_freq, &c->e_lanelen, &c->e_sinfo, &c->e_slab, &c->d_lit, &c->d_tok,
-                    &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->d_tot, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta, &c->work,
+                    &c->d_sym, &c->d_grp, &c->d_ext, &c->d_meta, &c->d_tks, &c->d_tkm, &c->d_tkd, &c->d_tkl, &c->s_in, &c->s_blk, &c->s_out, &c->s_meta, &c->work,
                     &c->a_desc, &c->a_work})
     release(*b);
   if (c->h_meta.p) cudaFreeHost(c->h_meta.p);
@@ -474,6 +489,7 @@ int zc_profile_stages(zc_ctx* c, uint32_t max, char* names, double* ms, uint64_t
 
 int zc_prepare(zc_ctx* c, uint32_t block_log, int level) {
   if (!c) return ZC_E_ARG;
+  ZC_GATE(c);
   if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
   c->block_log = block_log;
   c->level = level;
@@ -498,6 +514,7 @@ size_t zc_batch_bytes_decode(const zc_ctx*, uint32_t block_log) {
 int zc_compress(zc_ctx* c, const uint8_t* in, size_t n, uint32_t block_log, int level, uint8_t* methods,
                 uint32_t* comp_lens, uint32_t* crcs, uint8_t* payloads, size_t payload_cap, uint64_t* pay_offs) {
   if (!c) return ZC_E_ARG;
+  ZC_GATE(c);
   if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
   ZC_CUDA(cudaSetDevice(c->device));
   const uint64_t B = 1ull << block_log;
@@ -511,6 +528,7 @@ int zc_compress_batch(zc_ctx* c, const uint8_t* in, const uint64_t* in_offs, con
                       uint32_t block_log, int level, uint8_t* methods, uint32_t* comp_lens, uint32_t* crcs,
                       uint8_t* payloads, size_t payload_cap, uint64_t* pay_offs) {
   if (!c) return ZC_E_ARG;
+  ZC_GATE(c);
   if (nb && (!in_offs || !in_lens)) return fail(c, ZC_E_ARG, "block offsets and lengths are required");
   ZC_CUDA(cudaSetDevice(c->device));
   return compress_host(c, in, in_offs, in_lens, nb, 0, block_log, level, methods, comp_lens, crcs, payloads,
@@ -522,6 +540,7 @@ int zc_compress_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_in_offs
                        uint32_t* d_crcs, uint8_t* d_out, size_t out_cap, uint64_t* d_out_offs, uint64_t* d_total,
                        void* stream) {
   if (!c) return ZC_E_ARG;
+  ZC_GATE(c);
   ZC_CUDA(cudaSetDevice(c->device));
   if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
   if (nb > enc_blocks_per_launch(block_log)) return fail(c, ZC_E_ARG, "too many blocks for one launch");
@@ -540,6 +559,7 @@ int zc_decompress_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_com
                          const uint8_t* d_methods, const uint32_t* d_raw_lens, uint32_t nb, uint32_t block_log,
                          uint8_t* d_out, const uint64_t* d_out_offs, uint32_t* d_crcs, uint32_t* d_err, void* stream) {
   if (!c) return ZC_E_ARG;
+  ZC_GATE(c);
   ZC_CUDA(cudaSetDevice(c->device));
   if (nb > dec_blocks_per_launch(block_log)) return fail(c, ZC_E_ARG, "too many blocks for one launch");
   if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
@@ -596,6 +616,7 @@ int zc_set_shape(zc_ctx* c, uint32_t block_log, int level, const zc_shape* in) {
 // decoder's.  Each candidate runs once untimed and then `reps` times; its time is the smallest.
 int zc_autotune(zc_ctx* c, const uint8_t* sample, size_t n, uint32_t block_log, int level, zc_shape* chosen) {
   if (!c || (!sample && n)) return ZC_E_ARG;
+  ZC_GATE(c);
   if (bad_block_log(block_log)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
   if (!n) return fail(c, ZC_E_ARG, "autotuning needs a sample");
   ZC_CUDA(cudaSetDevice(c->device));
@@ -712,6 +733,7 @@ int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, con
                   const uint8_t* methods, const uint32_t* raw_lens, uint32_t nb, uint8_t* out, uint32_t* crcs_out,
                   uint32_t* block_err) {
   if (!c) return ZC_E_ARG;
+  ZC_GATE(c);
   ZC_CUDA(cudaSetDevice(c->device));
   uint32_t maxraw = 0;
   for (uint32_t b = 0; b < nb; ++b) maxraw = std::max(maxraw, raw_lens[b]);
@@ -826,6 +848,7 @@ int zc_decompress(zc_ctx* c, const uint8_t* comp, const uint64_t* comp_offs, con
 
 int zc_crc32(zc_ctx* c, const uint8_t* data, size_t n, uint32_t* crc) {
   if (!c || !crc) return ZC_E_ARG;
+  ZC_GATE(c);
   ZC_CUDA(cudaSetDevice(c->device));
   cudaStream_t st = c->stream;
   const size_t piece = (size_t)1 << 20;

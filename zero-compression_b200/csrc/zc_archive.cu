@@ -791,6 +791,7 @@ int zc_archive_write_device(zc_ctx* c, const uint8_t* d_solid, uint32_t block_lo
                             uint32_t n_entries, uint8_t* d_out, uint64_t out_cap, uint64_t* d_len,
                             uint32_t* d_entry_crcs, void* stream) {
   if (!c) return ZC_E_ARG;
+  ZC_GATE(c);
   ZC_CUDA(cudaSetDevice(c->device));
   return write_device(c, d_solid, block_log, level, entries, n_entries, d_out, out_cap, d_len, d_entry_crcs,
                       static_cast<cudaStream_t>(stream));
@@ -799,6 +800,7 @@ int zc_archive_write_device(zc_ctx* c, const uint8_t* d_solid, uint32_t block_lo
 int zc_archive_write(zc_ctx* c, const uint8_t* solid, uint32_t block_log, int level, zc_entry* entries,
                      uint32_t n_entries, uint8_t* out, uint64_t out_cap, uint64_t* out_len) {
   if (!c || !out_len) return ZC_E_ARG;
+  ZC_GATE(c);
   ZC_CUDA(cudaSetDevice(c->device));
   return write_host(c, solid, block_log, level, entries, n_entries, out, out_cap, out_len);
 }
@@ -828,6 +830,7 @@ int zc_archive_blocks(const uint8_t* arch, uint64_t len, const zc_archive_info* 
 
 int zc_archive_extract(zc_ctx* c, const uint8_t* arch, uint64_t len, uint8_t* out, uint64_t out_cap) {
   if (!c) return ZC_E_ARG;
+  ZC_GATE(c);
   ZC_CUDA(cudaSetDevice(c->device));
   return extract_host(c, arch, len, out, out_cap);
 }

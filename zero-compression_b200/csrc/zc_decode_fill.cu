@@ -202,8 +202,8 @@ __global__ void __launch_bounds__(1024, 2) k_dec_tokens(DecArgs A) {
   __syncthreads();
   if (tid == 0) {
     if (any_bad || op + (m.nl - li) != raw) flag(A.err, b, E_TOKEN);
-    A.tot_op[b] = op;
-    A.tot_li[b] = li;
+    A.meta[b].op_total = op;
+    A.meta[b].li_total = li;
   }
 }
 
@@ -330,7 +330,7 @@ __device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTab
   const uint32_t* Tm = A.tk_ms + (size_t)b * TC;
   const uint32_t* Td = A.tk_d + (size_t)b * TC;
   const uint32_t* Tl = A.tk_lik + (size_t)b * TC;
-  const uint32_t op_total = A.tot_op[b], li_total = A.tot_li[b];
+  const uint32_t op_total = m.op_total, li_total = m.li_total;
   // token windows: lane k holds token w0 + k of the current window, and of the next one (prefetched;
   // a match whose source lies beyond the ring has its first source line brought into L2 then)
   uint32_t w0 = 0;
@@ -410,9 +410,7 @@ cudaError_t prepare_fill() {
 
 void launch_decode_fill(const DecArgs& A, cudaStream_t st, Stages& S) {
   if (!A.nb) return;
-  S.begin("k_dec_streams", st);
-  launch_dec_streams(A, st);
-  S.end(st);
+  launch_dec_streams(A, st, S);
   S.begin("k_dec_tokens", st);
   k_dec_tokens<<<A.nb, 1024, 0, st>>>(A);
   S.end(st);

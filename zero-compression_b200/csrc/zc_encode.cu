@@ -15,8 +15,9 @@
 //                  per segment in parallel from the segment start, then re-walked from the true entry
 //                  until it meets the first walk (rounds until no segment exit moves); a warp's walks
 //                  step together and finish capped matches as a warp
-//   k_enc_streams  one warp per block: groups, recent offsets, tok / ext / sym / group streams, offset
-//                  bits (a warp-private bit window, no atomics on global memory), literals
+//   k_enc_streams  one warp per block: group starts from a running maximum of per-token thresholds and a
+//                  next-start chain, recent offsets by shuffles from each group's start, tok / ext / sym /
+//                  group streams, offset bits packed by a word-segmented OR-scan, literals
 //   k_enc_rans     one CTA per (block, stream): histogram, 12-bit normalisation with the reference's
 //                  tie-breaks, 64 lanes coding backwards (src/codec.h:41-147)
 //   k_enc_pack     one CTA per block: the payload (src/codec2.h:139-152), or "stored"
@@ -652,10 +653,26 @@ __device__ __forceinline__ void warp_copy_in(uint8_t* dst, const uint8_t* src, u
   if (lane < n - t) dst[t + lane] = src[t + lane];
 }
 
+// Tokens -> streams, one warp per block, 32 tokens a round (the next 32 loaded while these are coded).
+//
+// Groups follow the rule of src/codec2.h:103-116: a group ends before a token whose match source starts before
+// the token's own output and reaches past the group's first output byte, or once it holds 255 tokens.  Within
+// a round, a group opened at token g is read by token k exactly when the output start of g lies below k's
+// source reach, and the output starts rise with the token index; so each token k whose source starts before
+// its output gets theta_k = how many of the round's tokens start their output below its reach (at most k),
+// and a group opened at g ends at the first token with theta > g.  With P the running maximum of theta over
+// the round, that is next(g) = the first k with P_k > g: a binary search over P by shuffles.  The group open
+// when the round starts ends at the first token that reads it (or would be its 256th); the round's later group
+// starts follow from there by next().  A token's recent-offset symbols (250..252) name the offsets of the
+// three tokens before its group's first token (src/codec2.h:121-137).
+//
+// Offset bits (LSB first): each token's bits start at a running bit position.  The tokens are grouped by the
+// 32-bit output word their bits start in (the groups are runs of lanes), an OR-scan segmented by that word
+// collects each word's bits (64-bit values: a token's spill into the next word rides in the high half), and
+// the last lane of each run stores its completed word.  The partly filled last word carries to the next round.
 __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
-  const uint32_t w = threadIdx.x >> 5, lane = lane_id();
-  const uint32_t b = blockIdx.x * 4 + w;
-  __shared__ uint32_t win[4][24];
+  const uint32_t lane = lane_id();
+  const uint32_t b = blockIdx.x * 4 + (threadIdx.x >> 5);
   if (b >= A.nb) return;
   const uint32_t n = A.in_len[b], nt = A.bcnt[b * 8 + 0];
   const uint8_t* src = A.in + A.in_off[b];
@@ -669,12 +686,14 @@ __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
   uint8_t* grp = A.s_grp + (size_t)b * TC;
   uint8_t* ext = A.s_ext + (size_t)b * ext_cap(A.B);
   uint32_t* bitw = reinterpret_cast<uint32_t*>(A.s_bits + (size_t)b * bits_cap(A.B));
-  if (lane < 24) win[w][lane] = 0;
-  __syncwarp();
-  uint32_t op = 0, gstart = 0, gt = 0, ng = 0, ei = 0, li = 0;
-  uint64_t bp = 0, wbase = 0;
-  uint32_t r0 = 1, r1 = 4, r2 = 8, l0 = 1, l1 = 4, l2 = 8;
-  // tokens 32 at a time; the next 32 are loaded while these are coded
+  const uint32_t upto = 0xFFFFFFFFu >> (31u - lane);  // lanes 0 .. lane
+  uint32_t op = 0;                    // output end of the tokens coded so far
+  uint32_t gpos = 0, gcnt = 0;        // the open group: its first output byte, its tokens so far
+  uint32_t ra = 1, rb = 4, rc = 8;    // the open group's recent offsets
+  uint32_t pa = 1, pb = 4, pc = 8;    // the offsets of the last three tokens before the round, nearest first
+  uint32_t ng = 0, ei = 0, li = 0;
+  uint64_t bp = 0, wbase = 0;         // bits written so far; the first bit of the word being filled
+  uint32_t cw = 0;                    // that word's bits [wbase, bp)
   uint32_t ni = 0, nm = 4, nd = 1;
   if (lane < nt) { ni = TI[lane]; nm = TM[lane]; nd = TD[lane]; }
   for (uint32_t t0 = 0; t0 < nt; t0 += 32) {
@@ -684,59 +703,99 @@ __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
     const uint32_t i = ni, m = nm, d = nd;
     if (q + 32 < nt) { ni = TI[q + 32]; nm = TM[q + 32]; nd = TD[q + 32]; } else { ni = 0; nm = 4; nd = 1; }
     const uint32_t endk = i + m;
-    const uint32_t prev_end = __shfl_up_sync(kFull, endk, 1);
-    const uint32_t opk = lane == 0 ? op : prev_end;
+    const uint32_t up = __shfl_up_sync(kFull, endk, 1);
+    const uint32_t opk = lane == 0 ? op : up;
     const uint32_t L = on ? i - opk : 0u;
-    const uint32_t j = i - d, reach = j + min(m, d);
-    // groups (src/codec2.h:103-116): close at 255 tokens, or before a match that reads its own group
-    uint32_t sv = 0, lo = 0;
-    while (lo < c) {
-      const bool viol = on && lane >= lo &&
-                        ((j < opk && reach > gstart && !(lane == lo && gt == 0)) || gt + (lane - lo) >= kMaxGroup);
-      const unsigned vb = __ballot_sync(kFull, viol);
-      const uint32_t first = vb ? (uint32_t)__ffs(vb) - 1u : c;
-      if (lane >= lo && lane < first) sv = d == r0 ? kSymRep : d == r1 ? kSymRep + 1 : d == r2 ? kSymRep + 2 : bitlen(d);
-      for (uint32_t k = first > lo + 3 ? first - 3 : lo; k < first; ++k) {
-        const uint32_t v = __shfl_sync(kFull, d, k);
-        l2 = l1; l1 = l0; l0 = v;
-      }
-      gt += first - lo;
-      if (first < c) {
-        if (gt) { if (lane == 0) grp[ng] = (uint8_t)gt; ++ng; }
-        gt = 0;
-        gstart = __shfl_sync(kFull, opk, first);
-        r0 = l0; r1 = l1; r2 = l2;
-      }
-      lo = first;
+    const uint32_t reach = i - d + min(m, d);
+    const bool back = on && i - d < opk;  // the source starts before the token's own output
+    // theta: the round's tokens whose output starts below the reach (lanes past c compare as above all)
+    const uint32_t key = on ? opk : 0xFFFFFFFFu;
+    uint32_t below = 0;
+#pragma unroll
+    for (uint32_t s = 16; s; s >>= 1)
+      if (__shfl_sync(kFull, key, below + s - 1) < reach) below += s;
+    const uint32_t theta = back ? min(lane, below) : 0u;
+    // the open group ends at the first token that reads it, or that would be its 256th
+    const unsigned ends = __ballot_sync(kFull, on && ((back && reach > gpos) || gcnt + lane >= kMaxGroup));
+    const uint32_t s1 = ends ? (uint32_t)__ffs(ends) - 1u : c;
+    uint32_t pm = theta;  // running maximum of theta
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(kFull, pm, o);
+      if (lane >= o) pm = max(pm, v);
+    }
+    uint32_t nx = 0;  // next(lane): the first token with pm > lane (32: none)
+#pragma unroll
+    for (uint32_t s = 16; s; s >>= 1)
+      if (__shfl_sync(kFull, pm, nx + s - 1) <= lane) nx += s;
+    if (__shfl_sync(kFull, pm, nx) <= lane) nx = 32;
+    uint32_t starts = 0;  // the round's group starts (warp-uniform walk)
+    for (uint32_t s = s1; s < c; s = __shfl_sync(kFull, nx, s)) starts |= 1u << s;
+    // the token's group start gs (-1: the group open before the round) and its recent offsets
+    const uint32_t mine = starts & upto;
+    const int gs = mine ? 31 - __clz(mine) : -1;
+    const uint32_t x1 = __shfl_sync(kFull, d, max(gs - 1, 0)), x2 = __shfl_sync(kFull, d, max(gs - 2, 0)),
+                   x3 = __shfl_sync(kFull, d, max(gs - 3, 0));
+    uint32_t r0 = ra, r1 = rb, r2 = rc;
+    if (gs >= 0) {
+      r0 = gs >= 1 ? x1 : pa;
+      r1 = gs >= 2 ? x2 : gs == 1 ? pa : pb;
+      r2 = gs >= 3 ? x3 : gs == 2 ? pa : gs == 1 ? pb : pc;
+    }
+    const uint32_t sv = d == r0 ? kSymRep : d == r1 ? kSymRep + 1 : d == r2 ? kSymRep + 2 : bitlen(d);
+    // group counts: the open group's (when it ends in this round), then each start's that ends in it
+    const uint32_t open_ends = s1 < c && gcnt + s1 > 0 ? 1u : 0u;
+    if (lane == 0 && open_ends) grp[ng] = (uint8_t)(gcnt + s1);
+    if (((starts >> lane) & 1u) && nx < c) grp[ng + open_ends + __popc(mine) - 1] = (uint8_t)(nx - lane);
+    ng += open_ends + (starts ? (uint32_t)__popc(starts) - 1u : 0u);
+    if (starts) {
+      const uint32_t last = 31u - __clz(starts);
+      gpos = __shfl_sync(kFull, opk, last);
+      gcnt = c - last;
+      ra = __shfl_sync(kFull, r0, last);
+      rb = __shfl_sync(kFull, r1, last);
+      rc = __shfl_sync(kFull, r2, last);
+    } else {
+      gcnt += c;
+    }
+    {  // (only a full round is followed by another)
+      const uint32_t a = __shfl_sync(kFull, d, 31), bq = __shfl_sync(kFull, d, 30), cq = __shfl_sync(kFull, d, 29);
+      pa = a; pb = bq; pc = cq;
     }
     if (on) {
       tok[q] = (uint8_t)((min(L, 15u) << 4) | min(m - 4u, 15u));
       sym[q] = (uint8_t)sv;
     }
+    // ext bytes (src/codec2.h:120-121): L - 15 in 3 bytes when L >= 15, then m - 19 in 2 when m >= 19
     const uint32_t fl = on && L >= 15u, fm = on && m >= 19u;
-    const uint32_t nx = 3u * fl + 2u * fm;
-    const uint32_t xincl = warp_incl_scan(nx);
-    const uint32_t xq = ei + xincl - nx;
+    const uint32_t nx_b = 3u * fl + 2u * fm;
+    const uint32_t xincl = warp_incl_scan(nx_b);
+    const uint32_t xq = ei + xincl - nx_b;
     if (fl) { const uint32_t v = L - 15u; ext[xq] = (uint8_t)v; ext[xq + 1] = (uint8_t)(v >> 8); ext[xq + 2] = (uint8_t)(v >> 16); }
     if (fm) { const uint32_t v = m - 19u, y = xq + 3u * fl; ext[y] = (uint8_t)v; ext[y + 1] = (uint8_t)(v >> 8); }
-    // offset bits, LSB first, through the warp's window of 24 words
-    const uint32_t nbit = (on && sv < kSymRep) ? sv : 0u;
+    // offset bits
+    const uint32_t nbit = on && sv < kSymRep ? sv : 0u;
     const uint32_t bincl = warp_incl_scan(nbit);
-    if (nbit) {
-      const uint32_t val = d - (1u << nbit);
-      const uint32_t rel = (uint32_t)(bp + bincl - nbit - wbase);
-      const uint32_t sh = rel & 31u;
-      atomicOr(&win[w][rel >> 5], val << sh);
-      if (sh + nbit > 32u) atomicOr(&win[w][(rel >> 5) + 1], val >> (32u - sh));
+    const uint32_t rel = (uint32_t)(bp - wbase) + bincl - nbit;  // (bp - wbase < 32)
+    const uint32_t wi = rel >> 5;
+    uint64_t acc = nbit ? (uint64_t)(d - (1u << nbit)) << (rel & 31u) : 0ull;
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+      const uint64_t v = __shfl_up_sync(kFull, acc, o);
+      const uint32_t vw = __shfl_up_sync(kFull, wi, o);
+      if (lane >= o && vw == wi) acc |= v;
     }
-    __syncwarp();
+    const uint32_t rel_end = (uint32_t)(bp - wbase) + __shfl_sync(kFull, bincl, 31);
+    const uint32_t full = rel_end >> 5;  // words completed by this round
+    const uint32_t wprev = __shfl_up_sync(kFull, wi, 1), wnext = __shfl_down_sync(kFull, wi, 1);
+    const unsigned firsts = __ballot_sync(kFull, lane == 0 || wprev != wi);
+    const uint32_t f = 31u - __clz(firsts & upto);  // the first lane of this lane's run
+    const uint32_t spill = (uint32_t)(__shfl_sync(kFull, acc, f ? f - 1u : 0u) >> 32);
+    const uint32_t word = (uint32_t)acc | (f ? spill : 0u) | (wi == 0 ? cw : 0u);
+    if ((lane == 31 || wnext != wi) && wi < full) bitw[(wbase >> 5) + wi] = word;
+    const uint32_t w31 = __shfl_sync(kFull, word, 31), s31 = (uint32_t)(__shfl_sync(kFull, acc, 31) >> 32);
+    cw = __shfl_sync(kFull, wi, 31) == full ? w31 : s31;
     bp += __shfl_sync(kFull, bincl, 31);
-    const uint32_t full = (uint32_t)((bp - wbase) >> 5);
-    if (lane < full) bitw[(wbase >> 5) + lane] = win[w][lane];
-    const uint32_t carry = win[w][full];
-    __syncwarp();
-    if (lane < 24) win[w][lane] = lane == 0 ? carry : 0u;
-    __syncwarp();
     wbase += 32ull * full;
     // literals before each token: a lane copies its own short run; runs of kWarpCopyRun bytes or more
     // (a long incompressible stretch) are copied by the whole warp, one after another
@@ -746,19 +805,21 @@ __global__ void __launch_bounds__(128) k_enc_streams(EncArgs A) {
     if (!longrun)
       for (uint32_t k = 0; k < L; ++k) lit[lik + k] = src[opk + k];
     for (unsigned lb = __ballot_sync(kFull, longrun); lb; lb &= lb - 1) {
-      const uint32_t q = (uint32_t)__ffs(lb) - 1u;
-      const uint32_t qL = __shfl_sync(kFull, L, q), qd = __shfl_sync(kFull, lik, q), qs = __shfl_sync(kFull, opk, q);
-      warp_copy_in(lit + qd, src + qs, qL, lane);
+      const uint32_t r = (uint32_t)__ffs(lb) - 1u;
+      const uint32_t rL = __shfl_sync(kFull, L, r), rd = __shfl_sync(kFull, lik, r), rs = __shfl_sync(kFull, opk, r);
+      warp_copy_in(lit + rd, src + rs, rL, lane);
     }
     li += __shfl_sync(kFull, lincl, 31);
     ei += __shfl_sync(kFull, xincl, 31);
     op = __shfl_sync(kFull, endk, c - 1);
   }
-  if (gt && lane == 0) grp[ng] = (uint8_t)gt;
-  if (gt) ++ng;
+  if (gcnt) {
+    if (lane == 0) grp[ng] = (uint8_t)gcnt;
+    ++ng;
+  }
   warp_copy_in(lit + li, src + op, n - op, lane);
   li += n - op;
-  if (bp > wbase && lane == 0) bitw[wbase >> 5] = win[w][0];
+  if (bp > wbase && lane == 0) bitw[wbase >> 5] = cw;
   if (lane == 0) {
     A.bcnt[b * 8 + 1] = li;
     A.bcnt[b * 8 + 2] = ei;

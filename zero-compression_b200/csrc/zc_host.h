@@ -91,7 +91,7 @@ struct zc_ctx {
   zch::DevBuf e_tmp_pos, e_srt_pos, e_minfo, e_scnt, e_tk_seg, e_tmp_h, e_srt_h, e_tk_i, e_tk_m, e_tk_d, e_bcnt, e_lit, e_tok,
       e_ext, e_sym, e_grp, e_bits, e_lanes, e_freq, e_lanelen, e_sinfo, e_slab;
   // decoder scratch (likewise)
-  zch::DevBuf d_lit, d_tok, d_sym, d_grp, d_ext, d_meta, d_tks, d_tkm, d_tkd, d_tkl, d_tot;
+  zch::DevBuf d_lit, d_tok, d_sym, d_grp, d_ext, d_meta, d_tks, d_tkm, d_tkd, d_tkl;
   // staging for the host-pointer calls
   zch::DevBuf s_in, s_blk, s_out, s_meta;
   zch::HostBuf h_meta;
@@ -107,6 +107,9 @@ struct zc_ctx {
     cudaEvent_t ev_in = nullptr, ev_done = nullptr;
   } pipe[2];
   cudaStream_t cstream = nullptr;
+  // the test injector of device failures: ZC_FAIL_AFTER=n at open fails the (n+1)-th codec call
+  int64_t fail_after = -1;
+  bool lost = false;
 };
 
 namespace zch {
@@ -121,6 +124,8 @@ bool bad_block_log(uint32_t bl);
 uint32_t enc_blocks_per_launch(uint32_t block_log);
 uint32_t dec_blocks_per_launch(uint32_t block_log);
 int check_launch(zc_ctx* c, const char* what);
+// ZC_E_DEVICE when the injector fails this call (or failed an earlier one); counts the call otherwise
+int gate(zc_ctx* c);
 // the slice-by-8 tables and x^(8 * 2^e) powers of the CRC-32 (host copy; the context uploads one)
 void build_crc_tables(zc::CrcTables& T);
 // uniform blocks: block b of an n-byte span starts at b * B and holds min(B, n - b * B) bytes
@@ -138,6 +143,11 @@ int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs,
                   const uint64_t* d_out_offs, uint32_t* d_crcs, uint32_t* d_err, cudaStream_t st);
 
 }  // namespace zch
+
+#define ZC_GATE(c)                           \
+  do {                                       \
+    if (int g_ = zch::gate(c)) return g_;    \
+  } while (0)
 
 #define ZC_CUDA(call)                                  \
   do {                                                 \

@@ -19,8 +19,12 @@ struct Stages {
 };
 
 // ---- decoder
-struct DecMeta {  // per block: the payload's counts and where its offset bits start
-  uint32_t nt, nl, ne, nob, ng, bits_off;
+struct DecMeta {  // per block: the payload's framing (k_dec_locate) and the replay's totals (k_dec_tokens)
+  uint32_t nt, nl, ne, nob, ng;  // tokens, literals, ext bytes, offset-bit bytes, groups
+  uint32_t bits_off;             // where the offset bits start in the payload
+  uint32_t s_off[5], s_len[5];   // each stream body's offset in the payload and its length
+  uint32_t kinds;                // bit s: stream s is rANS-coded (else raw)
+  uint32_t op_total, li_total;   // output and literal bytes of all tokens (the literal tail follows)
 };
 
 struct DecArgs {
@@ -36,10 +40,8 @@ struct DecArgs {
   // scratch, per block slot b: lit at b*B, tok / sym / grp at b*tok_cap(B), ext at b*ext_cap(B)
   uint8_t *s_lit, *s_tok, *s_sym, *s_grp, *s_ext;
   DecMeta* meta;
-  // the two-kernel replay (launch_decode_fill) only: per token (tok_cap(B) per block) its output start,
-  // match start, offset and literal start; per block the output and literal totals of the tokens
+  // the replay: per token (tok_cap(B) per block) its output start, match start, offset and literal start
   uint32_t *tk_start, *tk_ms, *tk_d, *tk_lik;
-  uint32_t *tot_op, *tot_li;
   // the fill's shape: a ring of 2^ring_log recent output bytes per warp, fill_warps warps (blocks) per CTA
   uint32_t ring_log, fill_warps;
   uint32_t* work;             // the fill's device work counter (zeroed by the launcher)
@@ -60,8 +62,7 @@ struct CrcArgs {
   const CrcTables* tables;
 };
 
-void launch_decode(const DecArgs& A, cudaStream_t st, Stages& S);       // streams + one-kernel replay
-void launch_dec_streams(const DecArgs& A, cudaStream_t st);              // the rANS streams alone
+void launch_dec_streams(const DecArgs& A, cudaStream_t st, Stages& S);  // framing + the rANS streams
 void launch_decode_fill(const DecArgs& A, cudaStream_t st, Stages& S);  // streams + token scan + fill
 void launch_crc(const CrcArgs& A, cudaStream_t st, Stages& S, const char* name);
 
