@@ -822,10 +822,40 @@ def run_archive(args):
     return 0 if ok else 1
 
 
+def reference_archive(hv, bl, level):
+    """The CPU-baseline leg of the decode workload: the reference CPU codec (compiled from the reference's
+    sources, all host threads) writes the archive's records for the whole input, timed.  Returns
+    (methods, comp_lens, bodies blob, body offsets, seconds, threads), or None without the compiled
+    reference."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    if not O.Ref.available():
+        return None
+    B = 1 << bl
+    t0 = time.perf_counter()
+    methods, lens, pays = O.Ref.cpu_compress(hv, bl, O.depth_for_level(level))
+    dt = time.perf_counter() - t0
+    nb = len(methods)
+    clens = np.array([int(lens[b]) if methods[b] else min(B, hv.size - b * B) for b in range(nb)], np.int64)
+    coffs = np.concatenate([[0], np.cumsum(clens)[:-1]]).astype(np.int64)
+    blob = np.empty(int(clens.sum()) + 64, np.uint8)
+    for b in range(nb):
+        o = int(coffs[b])
+        if methods[b]:
+            blob[o:o + int(clens[b])] = np.frombuffer(pays[b], np.uint8)
+        else:
+            blob[o:o + int(clens[b])] = hv[b * B:b * B + int(clens[b])]
+    del pays
+    return methods.copy(), clens, blob, coffs, dt, O.Ref.hardware_threads()
+
+
 def run_decode(args):
-    """Decode-heavy workload (the decode config, scaled): LZ-mix data at block 2^20, level 9, compressed
-    once (untimed; the GPU encoder writes the reference CPU codec's bytes), then extracted K times.  Each
-    extract decodes every block and computes its CRC-32 (test = the same plus the comparison)."""
+    """Decode-heavy workload (the decode config): LZ-mix data at block 2^20, level 9.  The archive's records
+    are written by the reference CPU codec (the CPU-baseline leg, timed on the host's threads; without the
+    compiled reference, by the GPU encoder) and also by the GPU encoder, whose payloads must equal the
+    reference's for every block; then the reference-written records are extracted K times on the GPU.
+    Each extract decodes every block and computes its CRC-32 (test = the same plus the comparison)."""
     import numpy as np
     import torch
     import zero_cuda as Z
@@ -877,6 +907,34 @@ def run_decode(args):
     t_comp = time.perf_counter() - t0
     comp = int(clens.sum().item())
     dper = codec.batch_bytes_decode(bl) // B
+    writer, same, cpu = "GPU encoder", None, None
+    ref = None if args.no_cpu else reference_archive(hv, bl, level)
+    if ref is not None:
+        r_meth, r_clens, r_blob, r_coffs, r_dt, r_thr = ref
+        # the GPU encoder's records against the reference's, every block
+        g_meth = methods.cpu().numpy()
+        g_clens = clens.cpu().numpy().astype(np.int64)
+        g_offs = goffs.cpu().numpy()
+        same = bool(np.array_equal(g_meth, r_meth))
+        if same:
+            host_out = d_out.cpu().numpy()
+            for b in range(nb):
+                if r_meth[b] and (g_clens[b] != r_clens[b] or not np.array_equal(
+                        host_out[g_offs[b]:g_offs[b] + g_clens[b]], r_blob[r_coffs[b]:r_coffs[b] + r_clens[b]])):
+                    same = False
+                    break
+            del host_out
+        # the extract below decodes the reference-written records
+        d_out = torch.from_numpy(r_blob).to(dev)
+        goffs = torch.from_numpy(r_coffs).to(dev)
+        clens = torch.from_numpy(r_clens.astype(np.int32)).to(dev)
+        methods = torch.from_numpy(r_meth.astype(np.uint8)).to(dev)
+        comp = int(r_clens.sum())
+        writer = "reference CPU codec (oracle/_ref, the reference's own sources)"
+        cpu = {"value": round(n / r_dt / GB, 4), "unit": "GB/s", "cores": r_thr, "kind": "reference",
+               "sample": f"the whole {args.size_mib} MiB compressed at block {bl}, level {level} (the archive the "
+                         "GPU extracts)"}
+        del r_blob
 
     def decompress():
         for b0 in range(0, nb, dper):
@@ -884,6 +942,11 @@ def run_decode(args):
             codec.decompress_device(d_out, goffs[b0:], clens[b0:], methods[b0:], lens[b0:], k, bl, d_dec, offs[b0:],
                                     dcrcs[b0:], errs[b0:], stream=sh)
 
+    if args.fill_words or args.fill_ring_log or args.fill_warps:
+        kw = {k: v for k, v in (("fill_words", args.fill_words), ("fill_ring_log", args.fill_ring_log),
+                                ("fill_warps", args.fill_warps)) if v}
+        codec.set_shape(bl, level, **kw)
+    codec.prepare(bl)
     codec.set_graphs(True)
     for _ in range(args.warmup):
         decompress()
@@ -924,7 +987,10 @@ def run_decode(args):
                                      if dom[0] in DRAM_BYTES_PER_RAW_BYTE else None),
                          "pipeline_frac": round((n + comp) / (t * 1e-3) / GB / peak, 4)},
             "stages_ms_per_step": {k: round(v[0] / args.steps, 4) for k, v in stages.items()},
-            "gpu_launches": int(launches), "clocks": clk.summary()}
+            "gpu_launches": int(launches), "clocks": clk.summary(), "fill_shape": codec.get_shape(bl, level),
+            "archive_written_by": writer, "payloads_equal_reference_all_blocks": same}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     codec.close()
     return 0 if ok else 1
@@ -1051,6 +1117,9 @@ def main():
                     help="lz: the headline round trip; batched: many files, plain vs batched; decode: extract-heavy; "
                          "serve: the request loop; archive: whole .zero archives of many files; sweep: lz_mix at "
                          "block 16/18/20 x level 1/5/9 and random bytes")
+    ap.add_argument("--fill-words", type=int, default=0, help="decode: the fill's words a lane a round (1, 2, 4)")
+    ap.add_argument("--fill-ring-log", type=int, default=0, help="decode: the fill's ring size (log2 bytes)")
+    ap.add_argument("--fill-warps", type=int, default=0, help="decode: the fill's warps per CTA")
     ap.add_argument("--files", type=int, default=10000)
     ap.add_argument("--max-file-kib", type=int, default=1024)
     ap.add_argument("--pool", type=int, default=48, help="serve: distinct files the jobs draw from")

@@ -147,15 +147,17 @@ int zc_reserve(zc_ctx *ctx, uint32_t block_log, uint32_t nb);
  *   fill_ring_log   decoder fill: each warp keeps its last 2^fill_ring_log output bytes in shared memory
  *                   (11..15), so a match nearer than that reads shared instead of global memory
  *   fill_warps      decoder fill: blocks (warps) per CTA, 1, 2, 4 or 8; fill_warps * (2^fill_ring_log +
- *                   656) bytes of shared memory per CTA, at most 227 KiB
+ *                   1408 * fill_words) bytes of shared memory per CTA, at most 227 KiB
  *   match_cap       encoder match pass: bytes compared per candidate before the match is left to the
  *                   parse to finish, 8..32
  *   match_tile      encoder match pass: sorted positions per CTA of 256 threads (256, 512 or 1024)
+ *   fill_words      decoder fill: output words each lane fills per round (1, 2 or 4: rounds of 128,
+ *                   256 or 512 bytes, whose loads are in flight together)
  * The decoder uses the shape of the level last given to zc_prepare (5 by default).  zc_autotune times
  * the candidates on a host sample (its whole blocks, up to one encoder launch) and keeps the fastest for
  * (block_log, level); it allocates its own device buffers for the duration of the call. */
 typedef struct zc_shape {
-  uint32_t fill_ring_log, fill_warps, match_cap, match_tile;
+  uint32_t fill_ring_log, fill_warps, match_cap, match_tile, fill_words;
 } zc_shape;
 int zc_get_shape(const zc_ctx *ctx, uint32_t block_log, int level, zc_shape *out);
 int zc_set_shape(zc_ctx *ctx, uint32_t block_log, int level, const zc_shape *shape);

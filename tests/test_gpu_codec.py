@@ -252,12 +252,13 @@ def test_launch_shapes_never_change_bytes(codec):
             coffs = np.cumsum([0] + [len(c) for c in comp[:-1]])
             for rl in (11, 13, 15):
                 for w in (1, 2, 4, 8):
-                    if w * ((1 << rl) + 656) > 227 * 1024:
-                        continue
-                    codec.set_shape(bl, 5, fill_ring_log=rl, fill_warps=w)
-                    raw, dcrcs, errs = codec.decompress_arrays(b"".join(comp), coffs, [len(c) for c in comp],
-                                                               ref_m, raw_lens)
-                    assert not errs.any() and raw.tobytes() == data.tobytes(), (bl, rl, w)
+                    for wd in (1, 2, 4):
+                        if w * ((1 << rl) + 1408 * wd) > 227 * 1024:
+                            continue
+                        codec.set_shape(bl, 5, fill_ring_log=rl, fill_warps=w, fill_words=wd)
+                        raw, dcrcs, errs = codec.decompress_arrays(b"".join(comp), coffs, [len(c) for c in comp],
+                                                                   ref_m, raw_lens)
+                        assert not errs.any() and raw.tobytes() == data.tobytes(), (bl, rl, w, wd)
             chosen = codec.autotune(data, bl, 5)
             assert chosen == codec.get_shape(bl, 5)
             meth, lens, crcs, pay, offs = codec.compress_arrays(data, bl, level=5)

@@ -225,7 +225,7 @@ int decode_device(zc_ctx* c, const uint8_t* d_comp, const uint64_t* d_comp_offs,
   A.tk_start = c->d_tks.as<uint32_t>(); A.tk_ms = c->d_tkm.as<uint32_t>(); A.tk_d = c->d_tkd.as<uint32_t>();
   A.tk_lik = c->d_tkl.as<uint32_t>();
   const Shape& sh = c->shape[block_log - zc::kMinBlockLog][level_class(c->level)];
-  A.ring_log = sh.ring_log; A.fill_warps = sh.fill_warps;
+  A.ring_log = sh.ring_log; A.fill_warps = sh.fill_warps; A.fill_words = sh.fill_words;
   A.work = c->work.as<uint32_t>() + 1;
   zc::launch_decode_fill(A, st, c->stages);
   if (d_crcs && nb) {
@@ -589,6 +589,7 @@ int zc_get_shape(const zc_ctx* c, uint32_t block_log, int level, zc_shape* out) 
   out->fill_warps = s.fill_warps;
   out->match_cap = s.cmp_cap;
   out->match_tile = s.match_tile;
+  out->fill_words = s.fill_words;
   return ZC_OK;
 }
 
@@ -598,7 +599,8 @@ int zc_set_shape(zc_ctx* c, uint32_t block_log, int level, const zc_shape* in) {
   const uint32_t w = in->fill_warps;
   if (in->fill_ring_log < zc::kMinFillRingLog || in->fill_ring_log > zc::kMaxFillRingLog ||
       (w != 1 && w != 2 && w != 4 && w != 8) || in->match_cap < 8 ||
-      in->match_cap > 32 || zc::fill_smem_bytes(in->fill_ring_log, w) > zc::kMaxFillSmem ||
+      (in->fill_words != 1 && in->fill_words != 2 && in->fill_words != 4) ||
+      in->match_cap > 32 || zc::fill_smem_bytes(in->fill_ring_log, w, in->fill_words) > zc::kMaxFillSmem ||
       (in->match_tile != 256 && in->match_tile != 512 && in->match_tile != 1024))
     return fail(c, ZC_E_ARG, "launch shape out of range");
   ZC_CUDA(cudaSetDevice(c->device));
@@ -607,6 +609,7 @@ int zc_set_shape(zc_ctx* c, uint32_t block_log, int level, const zc_shape* in) {
   s.fill_warps = w;
   s.cmp_cap = in->match_cap;
   s.match_tile = in->match_tile;
+  s.fill_words = in->fill_words;
   drop_graphs(c);  // (captured launches carry the old shape)
   return ZC_OK;
 }
@@ -703,15 +706,16 @@ int zc_autotune(zc_ctx* c, const uint8_t* sample, size_t n, uint32_t block_log, 
     if ((r = encode())) break;  // (every cap writes the same payloads)
     best_ms = 1e30f;
     for (uint32_t rl = 11; rl <= 14 && !r; ++rl)
-      for (uint32_t w : {1u, 2u, 4u, 8u}) {
-        if (zc::fill_smem_bytes(rl, w) > zc::kMaxFillSmem) continue;
-        Shape s = best;
-        s.ring_log = rl; s.fill_warps = w;
-        cur = s;
-        float ms;
-        if ((r = timed(decode, ms))) break;
-        if (ms < best_ms) { best_ms = ms; best.ring_log = rl; best.fill_warps = w; }
-      }
+      for (uint32_t w : {1u, 2u, 4u, 8u})
+        for (uint32_t wd : {1u, 2u, 4u}) {
+          if (r || zc::fill_smem_bytes(rl, w, wd) > zc::kMaxFillSmem) continue;
+          Shape s = best;
+          s.ring_log = rl; s.fill_warps = w; s.fill_words = wd;
+          cur = s;
+          float ms;
+          if ((r = timed(decode, ms))) break;
+          if (ms < best_ms) { best_ms = ms; best.ring_log = rl; best.fill_warps = w; best.fill_words = wd; }
+        }
     if (r) break;
     cur = best;
   } while (false);

@@ -6,9 +6,10 @@
 //                 symbols (each names an earlier token's offset, src/codec2.h:180-192), resolved by pointer
 //                 jumping over all tokens at once.  Every check of the reference decoder is made here; a
 //                 failing one records a status and the block is not replayed.
-//   k_dec_fill    one warp per block: walks the groups in order and fills each group's output with all
-//                 lanes (a group's matches read only output from before the group, or their own
-//                 literals), the next 32 tokens' table loaded while the current ones are filled.
+//   k_dec_fill    one warp per block: fills the block in rounds of 128 output bytes (a 4-byte word a lane)
+//                 straight through, group boundaries or not: a byte whose source lies earlier in the same
+//                 round is passed along by shuffles once known; the token table is a 64-row ring in shared
+//                 memory, refilled 32 tokens at a time from registers loaded one window ahead.
 // Stored blocks are copied by k_dec_fill.  The rANS streams come from k_dec_streams (zc_decode.cu).
 #include <algorithm>
 
@@ -209,87 +210,22 @@ __global__ void __launch_bounds__(1024, 2) k_dec_tokens(DecArgs A) {
 
 namespace {
 
-// a chunk of at most 32 tokens of one group: start[i] the output start of token i (start[c] the chunk's
-// end); tk[i] = {match start, literal start - output start (mod 2^32), offset D, the reciprocal
-// ceil(2^32 / D) when the match overlaps itself (D < M, D >= 2), else 0}
+// The warp's token table: a ring of TR rows, token t in row t % TR.  start = the token's output start;
+// tk = {match start, literal start - output start (mod 2^32), offset D, the reciprocal ceil(2^32 / D)
+// for D >= 2 (0 for D = 1)}.  Token nt (one past the last) is the block's literal tail: it starts where
+// the tokens' output ends and is literals up to the block's end; later rows start at 0xFFFFFFFF.
+template <uint32_t TR>
 struct FillTable {
-  uint32_t start[33];
-  uint32_t pad_[3];
-  uint4 tk[32];
+  uint32_t start[TR];
+  uint4 tk[TR];
 };
-constexpr uint32_t kTableBytes = (sizeof(FillTable) + 15u) & ~15u;
+// per warp, for WPL output words a lane a round: the table's rows (a round's tokens and the one carried
+// in), its bytes, and the round's byte flags (which bytes are not known yet)
+__host__ __device__ constexpr uint32_t fill_rows(uint32_t wpl) { return 64 * wpl; }
+__host__ __device__ constexpr uint32_t fill_table_bytes(uint32_t wpl) { return 20 * fill_rows(wpl); }
+__host__ __device__ constexpr uint32_t fill_flag_bytes(uint32_t wpl) { return 128 * wpl; }
 
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
-
-// Fills [op, op_end) of the chunk's tokens, 4 bytes a lane per round of 128 bytes, each lane's word
-// aligned in memory.  A token is at least 4 bytes long, so an aligned word holds at most one token
-// start: a round's starts form a 32-bit word mask (one OR-reduction over the window lanes `cs` of
-// chunk tokens k0 .. k1-1), and a lane's bytes belong to the last token starting at or before its word,
-// or the one before that.  A byte is its token's literal, or a match byte whose source is output from
-// before the group or the token's own literals (an overlapping match, D < M, repeats the D bytes before
-// it: match byte i comes from ms - D + (i mod D), the quotient from a multiply-high by the reciprocal,
-// exact to one step, which a compare corrects).  Output from before the group is read from the warp's
-// ring of the last R output bytes (shared memory, indexed by address mod R) when the round's own stores
-// cannot have replaced it, else from global memory.  A round's loads are all issued before its stores.
-__device__ __forceinline__ void fill_span(const FillTable& T, uint8_t* o, uint8_t* ring, uint32_t rmask,
-                                          const uint8_t* lit, uint32_t op, uint32_t op_end, uint32_t cs, uint32_t k0,
-                                          uint32_t k1) {
-  const uint32_t lane = lane_id();
-  const uint32_t ob = (uint32_t)(uintptr_t)o;
-  const bool mine = lane >= k0 && lane < k1;
-  uint32_t kb = 0;  // chunk tokens starting before the round
-  for (int32_t base = (int32_t)op - (int32_t)((ob + op) & 3u); base < (int32_t)op_end; base += 128) {
-    const int32_t rel = (int32_t)cs - base;
-    const uint32_t mask = __reduce_or_sync(kFull, mine && rel >= 0 && rel < 128 ? 1u << (rel >> 2) : 0u);
-    const uint32_t cnt = kb + __popc(mask & (0xFFFFFFFFu >> (31u - lane)));
-    kb += __popc(mask);
-    const int32_t q0 = base + 4 * (int32_t)lane;
-    if (q0 >= (int32_t)op_end || q0 + 4 <= (int32_t)op) continue;
-    const int32_t b1 = base + 128 < (int32_t)op_end ? base + 128 : (int32_t)op_end;
-    const int32_t rlo = b1 - (int32_t)(rmask + 1);  // ring bytes at or after rlo survive this round's stores
-    const uint32_t i1 = cnt - 1, i0 = cnt >= 2 ? cnt - 2 : 0;
-    const uint32_t st1 = T.start[i1], st0 = T.start[i0];
-    const uint4 t1 = T.tk[i1], t0 = T.tk[i0];
-    const uint8_t* src[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const uint32_t q = (uint32_t)(q0 + j);
-      const bool h = q >= st1;
-      const uint32_t opk = h ? st1 : st0, ms = h ? t1.x : t0.x, ld = h ? t1.y : t0.y, D = h ? t1.z : t0.z,
-                     mg = h ? t1.w : t0.w;
-      const uint8_t* p;
-      if (q < ms) {
-        p = lit + (q + ld);
-      } else {
-        uint32_t s = q - D;
-        if (s >= ms) {
-          const uint32_t x = q - ms;
-          uint32_t r = mg ? x - __umulhi(x, mg) * D : 0u;
-          if ((int32_t)r < 0) r += D;
-          s = ms - D + r;
-        }
-        p = s >= opk ? lit + (s + ld) : (int32_t)s >= rlo ? ring + ((ob + s) & rmask) : o + s;
-      }
-      src[j] = (int32_t)q >= (int32_t)op && q < op_end ? p : ring;
-    }
-    uint32_t w = 0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) w |= (uint32_t)*src[j] << (8 * j);
-    uint8_t* rq = ring + ((ob + (uint32_t)q0) & rmask);
-    if (q0 >= (int32_t)op && q0 + 4 <= (int32_t)op_end) {
-      *reinterpret_cast<uint32_t*>(o + q0) = w;
-      *reinterpret_cast<uint32_t*>(rq) = w;
-    } else {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int32_t q = q0 + j;
-        if (q < (int32_t)op || q >= (int32_t)op_end) continue;
-        o[q] = (uint8_t)(w >> (8 * j));
-        rq[j] = (uint8_t)(w >> (8 * j));
-      }
-    }
-  }
-}
 
 __device__ inline void copy_bytes(uint8_t* d, const uint8_t* s, uint32_t n) {  // all lanes; no overlap
   const uint32_t l = lane_id();
@@ -307,9 +243,23 @@ __device__ inline void copy_bytes(uint8_t* d, const uint8_t* s, uint32_t n) {  /
 
 }  // namespace
 
-// The replay of block b by one warp, with the warp's table and ring.
-__device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTable& T, uint8_t* ring) {
-  const uint32_t R = 1u << A.ring_log;
+// The replay of block b by one warp, in rounds of 128 * WPL output bytes: WPL 128-byte lines of the output
+// address, lane k filling the aligned word at offset 4k of each.  Groups are not walked: a byte's value
+// comes from its token's literals, from output before the round (the warp's shared-memory ring of the last
+// R bytes, or global memory), or from an earlier byte of the same round.  The lanes first fill every byte
+// of the first two kinds with their loads in flight together; the bytes of the third kind then read their
+// sources from the round's words staged in the ring, pass after pass until all are known (each source lies
+// before its byte, so this ends; the format's groups keep those chains short).
+//
+// A token is at least 4 bytes long, so an aligned word holds at most one token start: a line's token
+// starts form a 32-bit word mask (one OR-reduction), and a lane's bytes belong to the last token starting at
+// or before its word's last byte, or the one before that.  A match byte's source is ms - D + ((q - ms) mod
+// D) (src/codec2.h:194-197: an overlapping match repeats its D bytes before it), the quotient from a
+// multiply-high by the reciprocal, exact to one step, which a compare corrects.
+template <uint32_t WPL, uint32_t TR>
+__device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTable<TR>& T, uint8_t* ring,
+                                           uint8_t* flags) {
+  const uint32_t R = 1u << A.ring_log, rmask = R - 1u;
   const uint32_t lane = lane_id();
   const uint32_t raw = A.raw_len[b], method = A.method[b], clen = A.comp_len[b], B = A.B;
   uint8_t* o = A.out + A.out_off[b];
@@ -322,90 +272,184 @@ __device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTab
   }
   if (method != 1) { if (lane == 0) flag(A.err, b, E_METHOD); return; }
   if (A.err[b]) return;
-  const DecMeta m = A.meta[b];
+  const DecMeta& m = A.meta[b];
+  const uint32_t nt = m.nt, op_total = m.op_total, li_total = m.li_total;
   const size_t TC = tok_cap(B);
   const uint8_t* lit = A.s_lit + (size_t)b * B;
-  const uint8_t* grp = A.s_grp + (size_t)b * TC;
   const uint32_t* Ts = A.tk_start + (size_t)b * TC;
   const uint32_t* Tm = A.tk_ms + (size_t)b * TC;
   const uint32_t* Td = A.tk_d + (size_t)b * TC;
   const uint32_t* Tl = A.tk_lik + (size_t)b * TC;
-  const uint32_t op_total = m.op_total, li_total = m.li_total;
-  // token windows: lane k holds token w0 + k of the current window, and of the next one (prefetched;
-  // a match whose source lies beyond the ring has its first source line brought into L2 then)
-  uint32_t w0 = 0;
-  auto load = [&](uint32_t base, uint32_t& s, uint32_t& ms, uint32_t& d, uint32_t& l) {
+  const uint32_t ob = (uint32_t)(uintptr_t)o;
+  // rows for tokens committed so far: [loaded - TR, loaded); row TR - 1 first holds a token "-1" (no byte
+  // uses it).  The next 32 tokens wait in registers (lane k: token loaded + k), fetched one window ahead;
+  // a match whose source lies beyond the ring has its first source lines brought into L2 then, and so
+  // does each token's first literal line.
+  uint32_t loaded = 0, ns, nm, nd, nl;
+  auto fetch = [&](uint32_t base) {
     const uint32_t t = base + lane;
-    if (t < m.nt) {
-      s = Ts[t]; ms = Tm[t]; d = Td[t]; l = Tl[t];
-      if (d >= R) prefetch_l2(o + (ms - d));
-    } else {
-      s = op_total; ms = op_total; d = 1; l = li_total;
+    ns = 0xFFFFFFFFu; nm = 0xFFFFFFFFu; nd = 1; nl = 0;
+    if (t < nt) {
+      ns = Ts[t]; nm = Tm[t]; nd = Td[t];
+      const uint32_t lk = Tl[t];
+      nl = lk - ns;
+      prefetch_l2(lit + lk);
+      if (nd >= R) {
+        prefetch_l2(o + (nm - nd));
+        prefetch_l2(o + (nm - nd) + 128);
+      }
+    } else if (t == nt) {
+      ns = op_total; nm = raw; nl = li_total - op_total;
     }
   };
-  uint32_t cs, cm, cd, cl, ns, nm, nd, nl;
-  load(0, cs, cm, cd, cl);
-  load(32, ns, nm, nd, nl);
-  const uint32_t rmask = R - 1;
-  uint32_t gc = 0;  // the group counts of groups gi0 .. gi0 + 31, lane k holding gi0 + k
-  uint32_t gi0 = 0, t = 0;
-  for (uint32_t g = 0; g < m.ng; ++g) {
-    if ((g & 31u) == 0) { gi0 = g; gc = g + lane < m.ng ? grp[g + lane] : 0u; }
-    const uint32_t gend = t + __shfl_sync(kFull, gc, g - gi0);
-    while (t < gend) {
-      if (t >= w0 + 32) {  // the next window becomes current; prefetch the one after
-        w0 += 32;
-        cs = ns; cm = nm; cd = nd; cl = nl;
-        load(w0 + 32, ns, nm, nd, nl);
-      }
-      const uint32_t k0 = t - w0, k1 = min(gend, w0 + 32) - w0, c = k1 - k0;
-      // each token's end: the next token's start (in this window or the next), or the total
-      const uint32_t e_next = __shfl_sync(kFull, ns, 0);
-      const uint32_t e_dn = __shfl_down_sync(kFull, cs, 1);
-      const uint32_t tend = lane < 31 ? e_dn : e_next;
-      if (lane >= k0 && lane < k1) {
-        const uint32_t i = lane - k0;
-        const uint32_t mg = cd >= 2 && cd < tend - cm ? 0xFFFFFFFFu / cd + 1u : 0u;
-        T.start[i] = cs;
-        T.tk[i] = make_uint4(cm, cl - cs, cd, mg);
-      }
-      const uint32_t op_end = __shfl_sync(kFull, tend, k1 - 1);
-      const uint32_t op = __shfl_sync(kFull, cs, k0);
-      if (lane == 0) T.start[c] = op_end;
+  auto commit = [&]() {
+    const uint32_t t = loaded + lane;
+    T.start[t % TR] = ns;
+    T.tk[t % TR] = make_uint4(nm, nl, nd, nd >= 2 ? 0xFFFFFFFFu / nd + 1u : 0u);
+    loaded += 32;
+    fetch(loaded);
+  };
+  fetch(0);
+  if (lane == 0) T.start[TR - 1] = 0;
+  commit();
+  __syncwarp();
+  uint32_t before = 0;  // tokens starting before the round
+  const uint32_t upto = 0xFFFFFFFFu >> (31u - lane);
+  for (int32_t lb = -(int32_t)(ob & 127u); lb < (int32_t)raw; lb += 128 * WPL) {
+    if (before + 32 * WPL > loaded) {  // (at most 32 tokens start in a line; the carried one keeps its row)
+      do commit(); while (before + 32 * WPL > loaded);
       __syncwarp();
-      fill_span(T, o, ring, rmask, lit, op, op_end, cs, k0, k1);
-      __syncwarp();
-      t += c;
     }
+    const int32_t rlo = lb - (int32_t)R;  // the ring holds output [lb - R, lb)
+    uint32_t w[WPL], pend = 0;            // pend: bit 4h + j, byte j of word h is not known yet
+    uint64_t srcs[WPL];                   // its source's offset in the round, 16 bits a byte
+    uint32_t bh = before;
+#pragma unroll
+    for (uint32_t h = 0; h < WPL; ++h) {
+      const int32_t lh = lb + 128 * (int32_t)h;
+      const uint32_t ts = T.start[(bh + lane) % TR];
+      const int32_t rel = (int32_t)(ts - (uint32_t)lh);
+      const uint32_t mask = __reduce_or_sync(kFull, ts != 0xFFFFFFFFu && rel >= 0 && rel < 128 ? 1u << (rel >> 2) : 0u);
+      const uint32_t t1 = bh + __popc(mask & upto) - 1u, t0 = t1 - 1u;  // (mod 2^32: token -1 is row TR - 1)
+      const uint32_t st1 = T.start[t1 % TR], st0 = T.start[t0 % TR];
+      const uint4 a1 = T.tk[t1 % TR], a0 = T.tk[t0 % TR];
+      bh += __popc(mask);
+      const int32_t q0 = lh + 4 * (int32_t)lane;
+      w[h] = 0;
+      srcs[h] = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int32_t qi = q0 + j;
+        if (qi < 0 || qi >= (int32_t)raw) continue;
+        const uint32_t q = (uint32_t)qi;
+        const bool hi = q >= st1;
+        const uint32_t opk = hi ? st1 : st0, ms = hi ? a1.x : a0.x, ld = hi ? a1.y : a0.y, D = hi ? a1.z : a0.z,
+                       mg = hi ? a1.w : a0.w;
+        uint32_t s = q;
+        if (q >= ms) {
+          const uint32_t x = q - ms;
+          uint32_t r = mg ? x - __umulhi(x, mg) * D : 0u;
+          if ((int32_t)r < 0) r += D;
+          s = ms - D + r;
+        }
+        const uint8_t* src;
+        if (s >= opk) {
+          src = lit + (s + ld);
+        } else if ((int32_t)s >= lb) {  // an earlier byte of this round
+          pend |= 1u << (4 * h + j);
+          srcs[h] |= (uint64_t)(s - (uint32_t)lb) << (16 * j);
+          continue;
+        } else {
+          src = (int32_t)s >= rlo ? ring + ((ob + s) & rmask) : o + s;
+        }
+        w[h] |= (uint32_t)*src << (8 * j);
+      }
+    }
+    // bytes from earlier in the round: the round's words staged in their ring slots (the ring's older
+    // bytes there are no longer needed: every load from the ring was made above), with a flag per byte
+    // still unknown; each pass takes the bytes whose sources are known
+    __syncwarp();  // (every lane's loads from the ring come before any lane's stores into it)
+    if (__any_sync(kFull, pend)) {
+      for (;;) {
+#pragma unroll
+        for (uint32_t h = 0; h < WPL; ++h) {
+          const uint32_t q0 = (uint32_t)(lb + 128 * (int32_t)h + 4 * (int32_t)lane);
+          *reinterpret_cast<uint32_t*>(ring + ((ob + q0) & rmask)) = w[h];
+          const uint32_t f = (pend >> (4 * h)) & 15u;
+          *reinterpret_cast<uint32_t*>(flags + 128 * h + 4 * lane) =
+              (f & 1u) | (f & 2u) << 7 | (f & 4u) << 14 | (f & 8u) << 21;
+        }
+        __syncwarp();
+        uint32_t left = pend;
+#pragma unroll
+        for (uint32_t h = 0; h < WPL; ++h) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            if (!((pend >> (4 * h + j)) & 1u)) continue;
+            const uint32_t sp = (uint32_t)(srcs[h] >> (16 * j)) & 0xFFFFu;
+            if (flags[sp]) continue;
+            w[h] |= (uint32_t)ring[(ob + (uint32_t)lb + sp) & rmask] << (8 * j);
+            left &= ~(1u << (4 * h + j));
+          }
+        }
+        pend = left;
+        __syncwarp();
+        if (!__any_sync(kFull, pend)) break;
+      }
+    }
+    // stores: the ring always whole words; the output whole words inside the block, bytes at its edges
+#pragma unroll
+    for (uint32_t h = 0; h < WPL; ++h) {
+      const int32_t q0 = lb + 128 * (int32_t)h + 4 * (int32_t)lane;
+      *reinterpret_cast<uint32_t*>(ring + ((ob + (uint32_t)q0) & rmask)) = w[h];
+      if (q0 >= 0 && q0 + 4 <= (int32_t)raw) {
+        *reinterpret_cast<uint32_t*>(o + q0) = w[h];
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (q0 + j >= 0 && q0 + j < (int32_t)raw) o[q0 + j] = (uint8_t)(w[h] >> (8 * j));
+      }
+    }
+    before = bh;
+    __syncwarp();
   }
-  copy_bytes(o + op_total, lit + li_total, m.nl - li_total);
 }
 
 // Fed by a device work queue: every warp takes the next block from the work counter until none is left,
-// so blocks of uneven sizes (a batch of many files) balance across warps.  A CTA holds blockDim.x / 32 warps, each
-// with its table and a ring of 2^ring_log bytes in dynamic shared memory (16-byte aligned, the ring after
-// the table).  The ring is read only at positions the warp has written in its current block.
+// so blocks of uneven sizes (a batch of many files) balance across warps.  A CTA holds blockDim.x / 32
+// warps, each with its table, a ring of 2^ring_log bytes and its byte flags in dynamic shared memory.
+// The ring is read only at positions the warp has written in its current block.
+template <uint32_t WPL>
 __global__ void __maxnreg__(72) k_dec_fill(DecArgs A) {  // (72 registers: 28 warps an SM with 4-warp CTAs)
+  constexpr uint32_t TR = fill_rows(WPL);
   extern __shared__ __align__(16) uint8_t fsm[];
   const uint32_t R = 1u << A.ring_log;
   const uint32_t wid = threadIdx.x >> 5;
-  FillTable& T = *reinterpret_cast<FillTable*>(fsm + (size_t)wid * (kTableBytes + R));
-  uint8_t* ring = fsm + (size_t)wid * (kTableBytes + R) + kTableBytes;
+  const size_t per = (size_t)fill_table_bytes(WPL) + R + fill_flag_bytes(WPL);
+  uint8_t* mine = fsm + (size_t)wid * per;
+  FillTable<TR>& T = *reinterpret_cast<FillTable<TR>*>(mine);
+  uint8_t* ring = mine + fill_table_bytes(WPL);
+  uint8_t* flags = ring + R;
   for (;;) {
     uint32_t b = 0;
     if (lane_id() == 0) b = atomicAdd(A.work, 1u);
     b = __shfl_sync(kFull, b, 0);
     if (b >= A.nb) break;
-    fill_block(A, b, T, ring);
+    fill_block<WPL>(A, b, T, ring, flags);
     __syncwarp();
   }
 }
 
-size_t fill_smem_bytes(uint32_t ring_log, uint32_t warps) { return (size_t)warps * (kTableBytes + (1u << ring_log)); }
+size_t fill_smem_bytes(uint32_t ring_log, uint32_t warps, uint32_t words) {
+  return (size_t)warps * (fill_table_bytes(words) + (1u << ring_log) + fill_flag_bytes(words));
+}
 
 cudaError_t prepare_fill() {
   const int cap = (int)kMaxFillSmem;
-  return cudaFuncSetAttribute(k_dec_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+  cudaError_t e = cudaFuncSetAttribute(k_dec_fill<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_dec_fill<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_dec_fill<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+  return e;
 }
 
 void launch_decode_fill(const DecArgs& A, cudaStream_t st, Stages& S) {
@@ -415,11 +459,13 @@ void launch_decode_fill(const DecArgs& A, cudaStream_t st, Stages& S) {
   k_dec_tokens<<<A.nb, 1024, 0, st>>>(A);
   S.end(st);
   const uint32_t W = A.fill_warps;
-  const size_t sm = fill_smem_bytes(A.ring_log, W);
+  const size_t sm = fill_smem_bytes(A.ring_log, W, A.fill_words);
   const uint32_t grid = (A.nb + W - 1) / W;  // (as many warps as blocks; the counter balances them)
   cudaMemsetAsync(A.work, 0, sizeof(uint32_t), st);
   S.begin("k_dec_fill", st);
-  k_dec_fill<<<grid, 32 * W, sm, st>>>(A);
+  if (A.fill_words == 4) k_dec_fill<4><<<grid, 32 * W, sm, st>>>(A);
+  else if (A.fill_words == 2) k_dec_fill<2><<<grid, 32 * W, sm, st>>>(A);
+  else k_dec_fill<1><<<grid, 32 * W, sm, st>>>(A);
   S.end(st);
 }
 

@@ -42,14 +42,15 @@ struct DecArgs {
   DecMeta* meta;
   // the replay: per token (tok_cap(B) per block) its output start, match start, offset and literal start
   uint32_t *tk_start, *tk_ms, *tk_d, *tk_lik;
-  // the fill's shape: a ring of 2^ring_log recent output bytes per warp, fill_warps warps (blocks) per CTA
-  uint32_t ring_log, fill_warps;
+  // the fill's shape: a ring of 2^ring_log recent output bytes per warp, fill_warps warps (blocks) per CTA,
+  // fill_words output words a lane a round (1, 2 or 4)
+  uint32_t ring_log, fill_warps, fill_words;
   uint32_t* work;             // the fill's device work counter (zeroed by the launcher)
 };
 
 constexpr uint32_t kMinFillRingLog = 11, kMaxFillRingLog = 15, kMaxFillWarps = 8;
 constexpr size_t kMaxFillSmem = 227 * 1024;
-size_t fill_smem_bytes(uint32_t ring_log, uint32_t warps);
+size_t fill_smem_bytes(uint32_t ring_log, uint32_t warps, uint32_t words);
 
 struct CrcArgs {
   const uint8_t* base;

@@ -137,9 +137,11 @@ extern "C" int zc_decompress_noalloc(const uint8_t* d_comp, const uint64_t* d_co
   A.tk_ms = reinterpret_cast<uint32_t*>(at); at += up256((size_t)nb * TC * 4);
   A.tk_d = reinterpret_cast<uint32_t*>(at); at += up256((size_t)nb * TC * 4);
   A.tk_lik = reinterpret_cast<uint32_t*>(at);
-  // the fill's launch shape: the default of the context-based calls (a ring of 4 KiB per warp, 4 warps a CTA)
+  // the fill's launch shape: the default of the context-based calls (a ring of 4 KiB per warp, 4 warps a
+  // CTA, a word a lane a round)
   A.ring_log = 12;
   A.fill_warps = 4;
+  A.fill_words = 1;
   zc::Stages stages;  // (no timing; nothing to record)
   zc::launch_decode_fill(A, st, stages);
   if (d_crcs) {
