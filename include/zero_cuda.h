@@ -269,6 +269,21 @@ int zc_archive_write_device(zc_ctx *ctx, const uint8_t *d_solid, uint32_t block_
                             const zc_entry *entries, uint32_t n_entries, uint8_t *d_out, uint64_t out_cap,
                             uint64_t *d_len, uint32_t *d_entry_crcs, void *stream);
 
+/* One rank's share of an archive written by several GPUs, one process each (no reference counterpart: the
+ * reference writes an archive from one process; the layout is compress_archive's, src/archive.h:389-403).
+ * d_range holds bytes [range_off, range_off + range_len) of the solid stream (device memory, 16-byte aligned,
+ * 64 readable bytes after its end); range_off is a multiple of 2^block_log, and so is the range's end unless
+ * it is the stream's end.  Writes the range's block records, exactly as zc_archive_write_device writes those
+ * blocks, into d_out from offset rec_base on (records only: no header, entry table or footer);
+ * out_cap - rec_base must hold 16 + 2^block_log bytes per block.  *d_len (device u64) gets rec_base plus the
+ * records' bytes; d_piece_crcs (device, n_entries; may be NULL) gets each entry's CRC-32 over its bytes
+ * inside the range (0 when it has none; the piece's length follows from the entries' sizes).  Combining
+ * the ranks' pieces in order with zc_crc32_combine gives each file's CRC.  Work is queued on `stream`. */
+int zc_archive_write_range(zc_ctx *ctx, const uint8_t *d_range, uint64_t range_off, uint64_t range_len,
+                           uint32_t block_log, int level, const zc_entry *entries, uint32_t n_entries,
+                           uint64_t rec_base, uint8_t *d_out, uint64_t out_cap, uint64_t *d_len,
+                           uint32_t *d_piece_crcs, void *stream);
+
 /* The same from host memory into host memory (synchronous): solid holds the files' bytes in entry order;
  * *out_len gets the archive's length and entries[i].crc each entry's CRC.  The stream goes through the GPU
  * in chunks (128 MiB, then 512 MiB): a chunk's upload and the previous chunk's records coming down

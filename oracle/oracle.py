@@ -233,7 +233,7 @@ class Ref(_Lib):
             raise RuntimeError(cls.last_error())
         pays = None
         if want_payloads:
-            pays = [out[b * stride: b * stride + lens[b]].tobytes() if methods[b] else None for b in range(nb)]
+            pays = [out[b * stride: b * stride + int(lens[b])].tobytes() if methods[b] else None for b in range(nb)]
         return methods[:nb], lens[:nb], pays
 
     @classmethod

@@ -45,6 +45,10 @@ __global__ void k_arch_head(Head h, uint8_t* out, uint64_t* rec_end0) {
   if (t == 0) *rec_end0 = kArchHdr;
 }
 
+// a range's records: the first record's position for the encoder's scan; then the end of the last record
+__global__ void k_range_start(uint64_t* rec_end0, uint64_t rec_base) { *rec_end0 = rec_base; }
+__global__ void k_range_end(const uint64_t* rec_end, uint64_t* out_len) { *out_len = *rec_end; }
+
 struct FileCrcArgs {
   uint32_t nf;               // files with bytes
   const uint32_t* first;     // nf + 1: file f's pieces are [first[f], first[f + 1])
@@ -185,6 +189,37 @@ bool cut_pieces(const zc_entry* es, uint32_t ne, uint32_t bl, uint64_t n, Pieces
       if (P.ref.size() >= 0xFFFFFFFFull || P.part_off.size() >= kPart) { why = "too many file pieces"; return false; }
     }
     at = e;
+  }
+  P.first.push_back((uint32_t)P.ref.size());
+  return true;
+}
+
+// The pieces of every file inside the stream range [lo, hi) (lo a multiple of the block size; hi too, or
+// the stream's end): blocks are numbered from the range's first, partial pieces' offsets count from lo.
+bool cut_range_pieces(const zc_entry* es, uint32_t ne, uint32_t bl, uint64_t lo, uint64_t hi, Pieces& P,
+                      std::string& why) {
+  const uint64_t B = 1ull << bl;
+  uint64_t at = 0;
+  for (uint32_t i = 0; i < ne; ++i) {
+    if (es[i].is_dir || !es[i].size) continue;
+    const uint64_t s = std::max(at, lo), e = std::min(at + es[i].size, hi);
+    at += es[i].size;
+    if (e <= s) continue;
+    P.first.push_back((uint32_t)P.ref.size());
+    P.entry.push_back(i);
+    for (uint64_t b = s >> bl; b <= (e - 1) >> bl; ++b) {
+      const uint64_t bs = b << bl, be = std::min(bs + B, hi);
+      const uint64_t ps = std::max(s, bs), pe = std::min(e, be);
+      if (ps == bs && pe == be) {
+        P.ref.push_back((uint32_t)(b - (lo >> bl)));
+      } else {
+        P.ref.push_back(kPart | (uint32_t)P.part_off.size());
+        P.part_off.push_back(ps - lo);
+        P.part_len.push_back((uint32_t)(pe - ps));
+      }
+      P.len.push_back((uint32_t)(pe - ps));
+      if (P.ref.size() >= 0xFFFFFFFFull || P.part_off.size() >= kPart) { why = "too many file pieces"; return false; }
+    }
   }
   P.first.push_back((uint32_t)P.ref.size());
   return true;
@@ -399,6 +434,66 @@ int write_device(zc_ctx* c, const uint8_t* d_solid, uint32_t bl, int level, cons
   k_arch_tail<<<grid, 1024, 0, st>>>(T);
   c->stages.end(st);
   return check_launch(c, "archive launch");
+}
+
+// One rank's share of a sharded archive: the block records of a range of the solid stream, from
+// rec_base on, and each file's CRC over its part of the range (the rank's piece of the file CRC).
+int write_range(zc_ctx* c, const uint8_t* d_range, uint64_t lo, uint64_t len, uint32_t bl, int level,
+                const zc_entry* es, uint32_t ne, uint64_t rec_base, uint8_t* d_out, uint64_t out_cap,
+                uint64_t* d_len, uint32_t* d_piece_crcs, cudaStream_t st) {
+  if (bad_block_log(bl)) return fail(c, ZC_E_ARG, "block size must be 2^16 .. 2^20 bytes");
+  std::string why;
+  uint64_t n = 0;
+  if (!check_entries(es, ne, &n, why)) return fail(c, ZC_E_ARG, why);
+  const uint64_t B = 1ull << bl, hi = lo + len;
+  if (lo & (B - 1) || hi > n || hi < lo || ((hi & (B - 1)) && hi != n))
+    return fail(c, ZC_E_ARG, "a range must start at a block boundary and end at one or at the stream's end");
+  if (len && (!d_range || ((uintptr_t)d_range & 15u))) return fail(c, ZC_E_ARG, "the range must be 16-byte aligned");
+  if (!d_out || !d_len) return fail(c, ZC_E_ARG, "no output");
+  const uint64_t nb64 = (len + B - 1) >> bl;
+  if (nb64 >= kPart) return fail(c, ZC_E_ARG, "too many blocks");
+  const uint32_t nb = (uint32_t)nb64;
+  if (out_cap < rec_base || out_cap - rec_base < nb64 * zc::kRecHdr + len)
+    return fail(c, ZC_E_ARG, "the output cannot hold the range's records (16 bytes + the block, each)");
+  Pieces P;
+  if (!cut_range_pieces(es, ne, bl, lo, hi, P, why)) return fail(c, ZC_E_ARG, why);
+  const uint32_t per = enc_blocks_per_launch(bl), nchunk = (nb + per - 1) / per;
+  Layout L;
+  const PieceDev pd = place_pieces(L, P, false);
+  std::vector<uint8_t> h(std::max<size_t>(L.at, 1));
+  fill_pieces(h, pd, P);
+  const uint32_t kmax = std::max(1u, std::min(nb, per));
+  Layout W;
+  const size_t o_meth = W.put(nb), o_lens = W.put(4ull * nb), o_crcs = W.put(4ull * nb), o_offs = W.put(8ull * nb);
+  const size_t o_ioff = W.put(8ull * kmax), o_ilen = W.put(4ull * kmax), o_pcrc = W.put(4 * P.part_off.size());
+  const size_t o_ends = W.put(8ull * (nchunk + 1));
+  ZC_CUDA(grow(c->a_desc, std::max<size_t>(L.at, 256)));
+  ZC_CUDA(grow(c->a_work, W.at));
+  uint8_t* D = c->a_desc.as<uint8_t>();
+  uint8_t* X = c->a_work.as<uint8_t>();
+  if (L.at) ZC_CUDA(cudaMemcpyAsync(D, h.data(), L.at, cudaMemcpyHostToDevice, st));
+  uint64_t* ends = reinterpret_cast<uint64_t*>(X + o_ends);
+  uint32_t* crcs = reinterpret_cast<uint32_t*>(X + o_crcs);
+  c->stages.begin("k_range_start", st);
+  k_range_start<<<1, 1, 0, st>>>(ends, rec_base);
+  c->stages.end(st);
+  for (uint32_t i = 0, b0 = 0; i < nchunk; ++i, b0 += per) {
+    const uint32_t k = std::min(per, nb - b0);
+    const uint64_t span = std::min<uint64_t>(len - (uint64_t)b0 * B, (uint64_t)k * B);
+    uint64_t* ioff = reinterpret_cast<uint64_t*>(X + o_ioff);
+    uint32_t* ilen = reinterpret_cast<uint32_t*>(X + o_ilen);
+    plain_blocks(c, span, (uint32_t)B, k, ioff, ilen, st);
+    if (int r = encode_device(c, d_range + (uint64_t)b0 * B, ioff, ilen, k, bl, level, X + o_meth + b0,
+                              reinterpret_cast<uint32_t*>(X + o_lens) + b0, crcs + b0, d_out, out_cap,
+                              reinterpret_cast<uint64_t*>(X + o_offs) + b0, ends + i + 1, 1, st, ends + i))
+      return r;
+  }
+  if (d_piece_crcs && ne) ZC_CUDA(cudaMemsetAsync(d_piece_crcs, 0, 4ull * ne, st));
+  launch_file_crcs(c, d_range, D, pd, P, crcs, reinterpret_cast<uint32_t*>(X + o_pcrc), nullptr, d_piece_crcs, st);
+  c->stages.begin("k_range_end", st);
+  k_range_end<<<1, 1, 0, st>>>(ends + nchunk, d_len);
+  c->stages.end(st);
+  return check_launch(c, "archive range launch");
 }
 
 int msg_fail(char* msg, size_t cap, const std::string& why) {
@@ -795,6 +890,16 @@ int zc_archive_write_device(zc_ctx* c, const uint8_t* d_solid, uint32_t block_lo
   ZC_CUDA(cudaSetDevice(c->device));
   return write_device(c, d_solid, block_log, level, entries, n_entries, d_out, out_cap, d_len, d_entry_crcs,
                       static_cast<cudaStream_t>(stream));
+}
+
+int zc_archive_write_range(zc_ctx* c, const uint8_t* d_range, uint64_t range_off, uint64_t range_len,
+                           uint32_t block_log, int level, const zc_entry* entries, uint32_t n_entries, uint64_t rec_base,
+                           uint8_t* d_out, uint64_t out_cap, uint64_t* d_len, uint32_t* d_piece_crcs, void* stream) {
+  if (!c) return ZC_E_ARG;
+  ZC_GATE(c);
+  ZC_CUDA(cudaSetDevice(c->device));
+  return write_range(c, d_range, range_off, range_len, block_log, level, entries, n_entries, rec_base, d_out, out_cap,
+                     d_len, d_piece_crcs, static_cast<cudaStream_t>(stream));
 }
 
 int zc_archive_write(zc_ctx* c, const uint8_t* solid, uint32_t block_log, int level, zc_entry* entries,

@@ -6,7 +6,8 @@ rank's total record bytes (16-byte block record + body, src/archive.h:389-403), 
 give each rank the offset of its first record.  CRCs of files that straddle two ranks' ranges combine
 with crc32::combine (src/crc32.h:60-66).  The exchange is one all-gather of one 64-bit value per rank
 (torch.distributed: NCCL between GPUs, gloo on the CPU), and, for the entry table, one all-gather of each
-rank's (crc, length) piece of every file.
+rank's (crc, length) piece of every file.  gpu_records writes a rank's records and file pieces on its GPU
+(zc_archive_write_range); records() builds them on the host from already coded blocks.
 """
 import struct
 
@@ -33,6 +34,32 @@ def records(raw, methods, comp_lens, crcs, bodies, block_log):
         out += struct.pack("<IIBBBBI", blk.size, len(body), 0 if stored else int(methods[b]), 0, 0, 0, int(crcs[b]))
         out += body
     return bytes(out)
+
+
+def gpu_records(codec, stream_range, range_off, entries, block_log, level=None):
+    """One rank's block records, written on its GPU by zc_archive_write_range: `stream_range` (numpy u8) is
+    the solid stream's bytes [range_off, range_off + len) -- whole blocks, the last may end the stream.
+    Returns (the records as bytes, per entry the (crc, length) of its piece inside the range)."""
+    import numpy as np
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n = int(stream_range.size)
+    B = 1 << block_log
+    nb = (n + B - 1) // B
+    d_range = torch.zeros(n + 64, dtype=torch.uint8, device=dev)
+    if n:
+        d_range[:n].copy_(torch.from_numpy(np.ascontiguousarray(stream_range)))
+    cap = nb * (REC_HDR + B) + 64
+    d_out = torch.zeros(cap, dtype=torch.uint8, device=dev)
+    d_len = torch.zeros(1, dtype=torch.int64, device=dev)
+    d_crc = torch.zeros(max(len(entries), 1), dtype=torch.int32, device=dev)
+    codec.archive_write_range(d_range, range_off, n, entries, block_log, d_out, d_len, d_crc, level=level)
+    torch.cuda.synchronize(dev)
+    length = int(d_len.item())
+    sizes = [0 if e.is_dir else e.size for e in entries]
+    lens = [ln for _, ln in file_pieces(sizes, range_off, range_off + n)]
+    crcs = [int(c) & 0xFFFFFFFF for c in d_crc.cpu().numpy()[:len(entries)]]
+    return d_out[:length].cpu().numpy().tobytes(), list(zip(crcs, lens))
 
 
 def place(local_bytes, group=None):

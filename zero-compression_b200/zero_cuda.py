@@ -96,6 +96,8 @@ def lib():
         L.zc_archive_write_device.argtypes = [_vp, _vp, C.c_uint32, C.c_int, _vp, C.c_uint32, _vp, C.c_uint64, _vp,
                                               _vp, _vp]
         L.zc_archive_write.argtypes = [_vp, _vp, C.c_uint32, C.c_int, _vp, C.c_uint32, _vp, C.c_uint64, _u64p]
+        L.zc_archive_write_range.argtypes = [_vp, _vp, C.c_uint64, C.c_uint64, C.c_uint32, C.c_int, _vp, C.c_uint32,
+                                             C.c_uint64, _vp, C.c_uint64, _vp, _vp, _vp]
         L.zc_archive_read_table.argtypes = [_vp, C.c_uint64, C.POINTER(ArchiveInfo), _vp, C.c_uint32, C.c_char_p,
                                             C.c_size_t]
         L.zc_archive_blocks.argtypes = [_vp, C.c_uint64, C.POINTER(ArchiveInfo), _vp, _vp, _vp, _vp, _vp, C.c_char_p,
@@ -573,6 +575,17 @@ class CudaCodec:
             self._ctx, _dp(d_solid), block_log, self.level if level is None else level, arr, len(entries),
             _dp(d_out), out_cap if out_cap is not None else d_out.numel(), _dp(d_len), _dp(d_entry_crcs),
             stream or None))
+
+    def archive_write_range(self, d_range, range_off, range_len, entries, block_log, d_out, d_len,
+                            d_piece_crcs=None, rec_base=0, stream=0, level=None, out_cap=None):
+        """zc_archive_write_range: one rank's block records of the stream range [range_off, range_off +
+        range_len) (in d_range) into d_out from rec_base on, *d_len = their end, d_piece_crcs[e] = entry e's
+        CRC over its bytes inside the range."""
+        arr, _keep = _c_entries(entries)
+        self._check(lib().zc_archive_write_range(
+            self._ctx, _dp(d_range), range_off, range_len, block_log, self.level if level is None else level, arr,
+            len(entries), rec_base, _dp(d_out), out_cap if out_cap is not None else d_out.numel(), _dp(d_len),
+            _dp(d_piece_crcs), stream or None))
 
     def archive_extract(self, arch, test=False):
         """Decodes and checks every block and file of an archive on the GPU (read_blocks + extract_archive /
