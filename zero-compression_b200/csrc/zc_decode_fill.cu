@@ -256,6 +256,9 @@ __device__ inline void copy_bytes(uint8_t* d, const uint8_t* s, uint32_t n) {  /
 // or before its word's last byte, or the one before that.  A match byte's source is ms - D + ((q - ms) mod
 // D) (src/codec2.h:194-197: an overlapping match repeats its D bytes before it), the quotient from a
 // multiply-high by the reciprocal, exact to one step, which a compare corrects.
+#ifndef ZC_FILL_BRANCHLESS
+#define ZC_FILL_BRANCHLESS 0
+#endif
 template <uint32_t WPL, uint32_t TR>
 __device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTable<TR>& T, uint8_t* ring,
                                            uint8_t* flags) {
@@ -338,6 +341,30 @@ __device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTab
       w[h] = 0;
       srcs[h] = 0;
 #pragma unroll
+#if ZC_FILL_BRANCHLESS
+      for (int j = 0; j < 4; ++j) {  // every choice a select, the load predicated
+        const int32_t qi = q0 + j;
+        const bool valid = qi >= 0 && qi < (int32_t)raw;
+        const uint32_t q = (uint32_t)qi;
+        const bool hi = q >= st1;
+        const uint32_t opk = hi ? st1 : st0, ms = hi ? a1.x : a0.x, ld = hi ? a1.y : a0.y, D = hi ? a1.z : a0.z,
+                       mg = hi ? a1.w : a0.w;
+        const uint32_t x = q - ms;
+        uint32_t r = x - __umulhi(x, mg) * D;
+        r = (int32_t)r < 0 ? r + D : r;
+        r = mg ? r : 0u;
+        const uint32_t s = q >= ms ? ms - D + r : q;
+        const bool own = s >= opk;
+        const bool inr = !own && (int32_t)s >= lb;
+        const uint8_t* src = own ? lit + (s + ld) : (int32_t)s >= rlo ? ring + ((ob + s) & rmask) : o + s;
+        const bool take = valid && inr;
+        pend |= (uint32_t)take << (4 * h + j);
+        srcs[h] |= take ? (uint64_t)(s - (uint32_t)lb) << (16 * j) : 0ull;
+        uint32_t v = 0;
+        if (valid && !inr) v = *src;
+        w[h] |= v << (8 * j);
+      }
+#else
       for (int j = 0; j < 4; ++j) {
         const int32_t qi = q0 + j;
         if (qi < 0 || qi >= (int32_t)raw) continue;
@@ -364,6 +391,7 @@ __device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTab
         }
         w[h] |= (uint32_t)*src << (8 * j);
       }
+#endif
     }
     // bytes from earlier in the round: the round's words staged in their ring slots (the ring's older
     // bytes there are no longer needed: every load from the ring was made above), with a flag per byte

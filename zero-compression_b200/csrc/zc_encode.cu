@@ -227,9 +227,6 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_sort_scatter(EncArgs A) {
 }
 
 // ---------------------------------------------------------------- 2. capped matches at every position
-#ifndef ZC_MATCH_HALF_WARPS
-#define ZC_MATCH_HALF_WARPS 0
-#endif
 // the first differing byte of two 16-byte windows (16 when equal)
 __device__ __forceinline__ uint32_t lcp16(const uint4& a0, const uint4& b0) {
   uint32_t x;
@@ -280,9 +277,7 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   uint32_t* spos = reinterpret_cast<uint32_t*>(win + NV * cap_e);
   uint16_t* sh = reinterpret_cast<uint16_t*>(spos + cap_e);
   uint32_t* wl = reinterpret_cast<uint32_t*>(sh + ((cap_e + 1) & ~1u));  // work list: entry | best << 16, distance
-#if !ZC_MATCH_HALF_WARPS
   const uint8_t* wb = reinterpret_cast<const uint8_t*>(win);
-#endif
   const uint32_t e0 = r0 > D ? r0 - D : 0, e1 = min(r0 + tile, count);
   const uint64_t base = A.in_off[b];
   const uint32_t* w32 = reinterpret_cast<const uint32_t*>(A.in);
@@ -335,64 +330,6 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   }
   __syncthreads();
   const uint32_t tw = nwork;
-#if ZC_MATCH_HALF_WARPS
-  // pass 2 over the work list, a half-warp per entry (a warp takes two entries at a time from a CTA
-  // counter): its 16 lanes compare 16 candidates of the entry's chain at once, the longest (capped) and
-  // nearest of them found by a max-reduction over (length, -candidate), which is the candidate the CPU
-  // walk keeps (src/codec2.h:58-67: strictly longer replaces, nearest first); a chunk whose best reaches the
-  // cap, or the chain's end, stops the entry.  The nearest candidate was compared in pass 1.
-  {
-    const uint32_t half = lane >> 4, hl = lane & 15u;
-    __shared__ uint32_t next2;
-    if (t == 0) next2 = 0;
-    __syncthreads();
-    for (;;) {
-      uint32_t w0 = 0;
-      if (lane == 0) w0 = atomicAdd(&next2, 2u);
-      w0 = __shfl_sync(kFull, w0, 0);
-      if (w0 >= tw) break;
-      const uint32_t my = w0 + half;
-      const bool have = my < tw;
-      uint32_t li = 0, l1 = 0, d1 = 0;
-      if (have) {
-        const uint32_t wa = wl[2 * my];
-        li = wa & 0xFFFFu;
-        l1 = wa >> 16;
-        d1 = wl[2 * my + 1];
-      }
-      const uint32_t r = li + e0, p = spos[li], h = sh[li];
-      const uint32_t lim = min(kMaxMatch, n - p), cap = min(min(A.cmp_cap, WB), lim);
-      const uint32_t kmax = min(D, r);
-      const uint4 p0 = win[NV * li], p1 = win[NV * li + NV - 1];
-      uint32_t key = (l1 << 16) | (0xFFFFu - 1u);  // candidate 1, from pass 1
-      bool go = have;
-      for (uint32_t kb = 2; __any_sync(kFull, go); kb += 16) {
-        const uint32_t k = kb + hl;
-        const bool valid = go && k <= kmax && sh[li - k] == h;
-        uint32_t c = 0;
-        if (valid) {
-          const uint32_t e = li - k;
-          const uint32_t l = min(NV == 2 ? lcp32(win[2 * e], win[2 * e + 1], p0, p1) : lcp16(win[e], p0), cap);
-          c = (l << 16) | (0xFFFFu - k);
-        }
-        key = max(key, c);
-#pragma unroll
-        for (uint32_t o = 8; o; o >>= 1) key = max(key, __shfl_xor_sync(kFull, key, o));
-        const bool any_valid = __ballot_sync(kFull, valid) & (0xFFFFu << (16 * half));
-        if (!any_valid || (key >> 16) == cap || kb + 16 > kmax) go = false;
-      }
-      if (have && hl == 0) {
-        const uint32_t l = key >> 16, k = 0xFFFFu - (key & 0xFFFFu);
-        uint32_t v;
-        if (l < 4) v = M_NONE;
-        else if (l == cap && cap < lim) v = M_SAT | r;
-        else v = m_pack(l, k == 1 ? d1 : p - spos[li - k]);
-        A.minfo[so + p] = v;
-      }
-    }
-  }
-}
-#else
   // pass 2 over the work list, lanes taking entries from a CTA counter.  Per-lane state: the position's
   // entry li, its chain of kend earlier entries with the same hash (found by a binary search: the
   // entries are sorted by hash), the candidate k reached so far, the best length, its distance, and the
@@ -467,7 +404,6 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
     }
   }
 }
-#endif
 
 // ---------------------------------------------------------------- 3. the parse
 struct ParseBlock {
@@ -563,62 +499,9 @@ __device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x) {
   return e;
 }
 
-// 16 bytes at byte offset a of the input, any alignment: five aligned words, funnel-shifted (they may reach
-// 19 bytes past a, inside the input's readable slack)
-__device__ __forceinline__ uint4 load16(const uint8_t* in, uint64_t a) {
-  const uint32_t* w = reinterpret_cast<const uint32_t*>(in) + (a >> 2);
-  const uint32_t s = (uint32_t)(a & 3u) * 8u;
-  const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3), w4 = __ldg(w + 4);
-  return make_uint4(__funnelshift_r(w0, w1, s), __funnelshift_r(w1, w2, s), __funnelshift_r(w2, w3, s),
-                    __funnelshift_r(w3, w4, s));
-}
-
-// The exact match at x by one lane alone: the CPU parse's chain walk (src/codec2.h:58-67) over the entries
-// before x's index r in the hash-sorted order, nearest first, at most `depth` of them: a candidate whose byte
-// at the current best length differs from x's cannot be longer and is passed over after one byte compare;
-// the others are compared 16 bytes a step.  The longest wins, the nearest on a tie.  Writes the exact record
-// over the capped one in minfo (a record already finished by another walk is rewritten with the same value).
-__device__ uint32_t lane_exact(const ParseBlock& P, uint32_t x, uint32_t v) {
-  const uint32_t r = v & 0xFFFFFu, h = P.sh[r];
-  const uint32_t lim = min(kMaxMatch, P.n - x), kmax = min(P.depth, r);
-  const uint64_t ax = P.base + x;
-  const uint4 xw = load16(P.in, ax);
-  uint32_t best = 0, bd = 0;
-  for (uint32_t k = 1; k <= kmax; ++k) {
-    const uint32_t e = r - k;
-    if (P.sh[e] != h) break;
-    const uint32_t j = P.spos[e];
-    const uint64_t aj = P.base + j;
-    if (best) {
-      const uint32_t q = min(best, lim - 1u);
-      if (__ldg(P.in + aj + q) != __ldg(P.in + ax + q)) continue;
-    }
-    uint32_t l = lcp16(load16(P.in, aj), xw);
-    if (l == 16u) {
-      while (l < lim) {
-        const uint32_t m = lcp16(load16(P.in, aj + l), load16(P.in, ax + l));
-        l += m;
-        if (m < 16u) break;
-      }
-    }
-    l = min(l, lim);
-    if (l > best) { best = l; bd = x - j; }
-  }
-  const uint32_t e = m_pack(best, bd);  // (a capped record's chain holds a match of at least the cap, >= 8)
-  P.minfo[x] = e;
-  return e;
-}
-
-// Capped records are finished by the whole warp, one at a time (coop_exact), when few lanes of a step hold
-// one; from this many on, each lane finishes its own (lane_exact) and the lanes' walks run side by side.
-#ifndef ZC_LANE_FINISH_MIN
-#define ZC_LANE_FINISH_MIN 4
-#endif
-constexpr int kLaneFinishMin = ZC_LANE_FINISH_MIN;
-
 // One step of the CPU parse (src/codec2.h:69-80) for every lane with `act` (all 32 lanes call it):
 // returns the next position (p itself when !act); the token, when the step emits one, in (ti, tm, td).
-// Capped records at p or p + 1 are finished first (by the whole warp, or by their own lanes).  A position with
+// Capped records at p or p + 1 are finished first, one at a time, by the whole warp.  A position with
 // no match is a literal step to the next position, so a run of them is taken at once, up to `lim` (the
 // walk's end): the walk lands where the CPU parse's single steps would first leave the run or reach lim.
 __device__ __forceinline__ uint32_t warp_step(const ParseBlock& P, uint32_t p, uint32_t lim, bool act, bool& tok,
@@ -627,18 +510,13 @@ __device__ __forceinline__ uint32_t warp_step(const ParseBlock& P, uint32_t p, u
   const bool lz = act && v != M_NONE && p + 1 < P.n;
   uint32_t v2 = lz ? P.minfo[p + 1] : M_NONE;
   unsigned s1 = __ballot_sync(kFull, act && m_is_sat(v));
-  unsigned s2 = __ballot_sync(kFull, lz && m_is_sat(v2));
-  if (__popc(s1) + __popc(s2) >= kLaneFinishMin) {
-    if ((s1 >> lane_id()) & 1u) v = lane_exact(P, p, v);
-    if ((s2 >> lane_id()) & 1u) v2 = lane_exact(P, p + 1u, v2);
-    s1 = s2 = 0;
-  }
   while (s1) {
     const uint32_t L = (uint32_t)__ffs(s1) - 1u;
     s1 &= s1 - 1u;
     const uint32_t e = coop_exact(P, __shfl_sync(kFull, p, L));
     if (lane_id() == L) v = e;
   }
+  unsigned s2 = __ballot_sync(kFull, lz && m_is_sat(v2));
   while (s2) {
     const uint32_t L = (uint32_t)__ffs(s2) - 1u;
     s2 &= s2 - 1u;
