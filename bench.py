@@ -32,10 +32,10 @@ sys.path.insert(0, os.path.join(ROOT, "zero-compression_b200"))
 
 METRIC = "compress/decompress GB/s on 1 B200, bit-exact round-trip; served p50/p99 latency"
 # dram__bytes_read.sum + dram__bytes_write.sum per raw byte of one launch (block 18, level 5 lz_mix), from
-# the ncu captures summarised in profiles/encoder_kernels_lz256m_b18_l5.md (256 MiB launch) and
-# profiles/decoder_kernels_lz512m_b18_l5.md (512 MiB launch)
+# the ncu captures summarised in profiles/encoder_kernels_lz256m_b18_l5.md (256 MiB launch),
+# profiles/decoder_fill_lz512m_b18_l5.md (512 MiB launch) and profiles/decoder_kernels_lz256m_b18_l5.md
 DRAM_BYTES_PER_RAW_BYTE = {"k_enc_match": 10.893, "k_enc_parse": 24.74, "k_sort_scatter": 9.81,
-                           "k_dec_fill": 1.762, "k_dec_tokens": 0.278, "k_dec_streams": 0.278}
+                           "k_dec_fill": 2.084, "k_dec_tokens": 0.186, "k_dec_streams": 0.198}
 GB = 1e9
 
 

@@ -256,9 +256,6 @@ __device__ inline void copy_bytes(uint8_t* d, const uint8_t* s, uint32_t n) {  /
 // or before its word's last byte, or the one before that.  A match byte's source is ms - D + ((q - ms) mod
 // D) (src/codec2.h:194-197: an overlapping match repeats its D bytes before it), the quotient from a
 // multiply-high by the reciprocal, exact to one step, which a compare corrects.
-#ifndef ZC_FILL_BRANCHLESS
-#define ZC_FILL_BRANCHLESS 0
-#endif
 template <uint32_t WPL, uint32_t TR>
 __device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTable<TR>& T, uint8_t* ring,
                                            uint8_t* flags) {
@@ -341,7 +338,6 @@ __device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTab
       w[h] = 0;
       srcs[h] = 0;
 #pragma unroll
-#if ZC_FILL_BRANCHLESS
       for (int j = 0; j < 4; ++j) {  // every choice a select, the load predicated
         const int32_t qi = q0 + j;
         const bool valid = qi >= 0 && qi < (int32_t)raw;
@@ -364,34 +360,6 @@ __device__ __forceinline__ void fill_block(const DecArgs& A, uint32_t b, FillTab
         if (valid && !inr) v = *src;
         w[h] |= v << (8 * j);
       }
-#else
-      for (int j = 0; j < 4; ++j) {
-        const int32_t qi = q0 + j;
-        if (qi < 0 || qi >= (int32_t)raw) continue;
-        const uint32_t q = (uint32_t)qi;
-        const bool hi = q >= st1;
-        const uint32_t opk = hi ? st1 : st0, ms = hi ? a1.x : a0.x, ld = hi ? a1.y : a0.y, D = hi ? a1.z : a0.z,
-                       mg = hi ? a1.w : a0.w;
-        uint32_t s = q;
-        if (q >= ms) {
-          const uint32_t x = q - ms;
-          uint32_t r = mg ? x - __umulhi(x, mg) * D : 0u;
-          if ((int32_t)r < 0) r += D;
-          s = ms - D + r;
-        }
-        const uint8_t* src;
-        if (s >= opk) {
-          src = lit + (s + ld);
-        } else if ((int32_t)s >= lb) {  // an earlier byte of this round
-          pend |= 1u << (4 * h + j);
-          srcs[h] |= (uint64_t)(s - (uint32_t)lb) << (16 * j);
-          continue;
-        } else {
-          src = (int32_t)s >= rlo ? ring + ((ob + s) & rmask) : o + s;
-        }
-        w[h] |= (uint32_t)*src << (8 * j);
-      }
-#endif
     }
     // bytes from earlier in the round: the round's words staged in their ring slots (the ring's older
     // bytes there are no longer needed: every load from the ring was made above), with a flag per byte
