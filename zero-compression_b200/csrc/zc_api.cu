@@ -130,7 +130,7 @@ int ensure_enc(zc_ctx* c, uint32_t nb, uint32_t block_log) {
       {&c->e_bcnt, (size_t)nb * 8 * 4}, {&c->e_lit, N}, {&c->e_tok, nb * TC}, {&c->e_ext, nb * EC},
       {&c->e_sym, nb * TC}, {&c->e_grp, nb * TC}, {&c->e_bits, (size_t)nb * zc::bits_cap((uint32_t)B)},
       {&c->e_lanes, (size_t)nb * zc::lanes_per_block((uint32_t)B)}, {&c->e_freq, (size_t)nb * 5 * 256 * 2},
-      {&c->e_lanelen, (size_t)nb * 5 * 64 * 4}, {&c->e_sinfo, (size_t)nb * 5 * 4 * 4}, {&c->e_slab, N}};
+      {&c->e_lanelen, (size_t)nb * 5 * 64 * 4}, {&c->e_sinfo, (size_t)nb * 5 * 4 * 4}, {&c->e_slab, N + 64}};
   return ensure(c, need);
 }
 

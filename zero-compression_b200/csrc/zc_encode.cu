@@ -1122,6 +1122,22 @@ __global__ void __launch_bounds__(256) k_enc_emit(EncArgs A) {
     for (uint32_t v = threadIdx.x; v < nvec; v += blockDim.x)
       reinterpret_cast<uint4*>(d + i)[v] = reinterpret_cast<const uint4*>(s + i)[v];
     i += nvec * 16;
+  } else {
+    // not co-aligned (every record of an archive): 4-byte words stored aligned at d, each built by a funnel
+    // shift from the two aligned source words that cover it (those reach at most 3 bytes past the body,
+    // inside the input's slack or the slab's padding)
+    const uint32_t head = min(len, (uint32_t)((4u - ((uintptr_t)d & 3u)) & 3u));
+    if (threadIdx.x < head) d[threadIdx.x] = s[threadIdx.x];
+    i = head;
+    const uint32_t nw = (len - i) >> 2, sh = (uint32_t)((uintptr_t)(s + i) & 3u);
+    const uint32_t* sw = reinterpret_cast<const uint32_t*>(s + i - sh);
+    uint32_t* dw = reinterpret_cast<uint32_t*>(d + i);
+    if (sh == 0) {
+      for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) dw[w] = sw[w];
+    } else {
+      for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) dw[w] = __funnelshift_r(sw[w], sw[w + 1], 8u * sh);
+    }
+    i += nw * 4;
   }
   for (uint32_t k = i + threadIdx.x; k < len; k += blockDim.x) d[k] = s[k];
 }
