@@ -27,8 +27,9 @@
 
 namespace zc {
 
-// per-position match record: NONE; SAT | r (a candidate reached cmp_cap; r is the position's index in the
-// hash-sorted order, where its chain starts: finished on demand by the parse); or the exact
+// per-position match record: NONE; SAT | r (a candidate reached cmp_cap, or the position lies inside a
+// longer match that starts before it; r is the position's index in the hash-sorted order, where its chain
+// starts: finished on demand by the parse, which computes the chain's exact best); or the exact
 // (length - 4) << 20 | (distance - 1).  Lengths are <= 4096, so an exact record never has 0xFFF in its
 // top 12 bits, and r < 2^20 - 3, so SAT | r is never NONE.
 constexpr uint32_t M_NONE = 0xFFFFFFFFu;
@@ -227,6 +228,15 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_sort_scatter(EncArgs A) {
 }
 
 // ---------------------------------------------------------------- 2. capped matches at every position
+// A position whose nearest candidate matches at least 4 bytes and also the kDeferBack bytes before them is
+// inside a longer match; the match pass leaves it to the parse (1..4 bytes; the mask selects them in the
+// little-endian word of the 4 bytes before the position)
+#ifndef ZC_DEFER_BACK
+#define ZC_DEFER_BACK 3
+#endif
+constexpr uint32_t kDeferBack = ZC_DEFER_BACK;
+constexpr uint32_t kDeferBackMask = 0xFFFFFFFFu << (8u * (4u - kDeferBack));
+
 // the first differing byte of two 16-byte windows (16 when equal)
 __device__ __forceinline__ uint32_t lcp16(const uint4& a0, const uint4& b0) {
   uint32_t x;
@@ -280,19 +290,29 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   const uint8_t* wb = reinterpret_cast<const uint8_t*>(win);
   const uint32_t e0 = r0 > D ? r0 - D : 0, e1 = min(r0 + tile, count);
   const uint64_t base = A.in_off[b];
-  const uint32_t* w32 = reinterpret_cast<const uint32_t*>(A.in);
-  const uint64_t wend = (base + n + 3) >> 2;  // words at or past it are not read (they lie past the block)
+  // (a window may reach up to WB + 15 bytes past its position, inside the input's readable slack; bytes past
+  // the block never decide a match: every compare is capped at the block's end)
   if (t == 0) { next = 0; nwork = 0; }
   for (uint32_t i = t; e0 + i < e1; i += 256) {
     const uint32_t r = e0 + i;
     const uint32_t p = A.srt_pos[so + r];
     spos[i] = p;
     sh[i] = A.srt_h[so + r];
-    const uint64_t a = base + p, wa = a >> 2;
-    const uint32_t shf = (uint32_t)(a & 3u) * 8u;
+    // the window from WB / 16 + 1 aligned 16-byte loads (a few L1 requests an entry instead of one a word:
+    // the entries' positions are scattered), its words picked by selects on the word offset
+    const uint64_t a = base + p;
+    const uint4* c = reinterpret_cast<const uint4*>(A.in + (a & ~(uint64_t)15));
+    constexpr uint32_t NC = WB / 16 + 1;
+    uint32_t cw[4 * NC];
+#pragma unroll
+    for (uint32_t k = 0; k < NC; ++k) {
+      const uint4 x = __ldg(c + k);
+      cw[4 * k] = x.x; cw[4 * k + 1] = x.y; cw[4 * k + 2] = x.z; cw[4 * k + 3] = x.w;
+    }
+    const uint32_t o = (uint32_t)(a >> 2) & 3u, shf = (uint32_t)(a & 3u) * 8u;
     uint32_t w[WB / 4 + 1];
 #pragma unroll
-    for (uint32_t q = 0; q <= WB / 4; ++q) w[q] = wa + q < wend ? __ldg(w32 + wa + q) : 0u;
+    for (uint32_t q = 0; q <= WB / 4; ++q) w[q] = o == 0 ? cw[q] : o == 1 ? cw[q + 1] : o == 2 ? cw[q + 2] : cw[q + 3];
     uint32_t v[WB / 4];
 #pragma unroll
     for (uint32_t q = 0; q < WB / 4; ++q) v[q] = __funnelshift_r(w[q], w[q + 1], shf);
@@ -319,6 +339,12 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
         v = cap < lim ? M_SAT | r : m_pack(l, d);
       } else if (r < 2 || D < 2 || sh[li - 2] != h) {
         v = l < 4 ? M_NONE : m_pack(l, d);
+      } else if (l >= 4 && p >= 4 && p - d >= 4 &&
+                 ((load4(A.in, base + p - 4) ^ load4(A.in, base + p - d - 4)) & kDeferBackMask) == 0) {
+        // the nearest candidate's match also runs kDeferBack bytes back, so p lies inside a longer match
+        // that starts earlier: the parse rarely visits it (it lands on match starts and the position after
+        // them).  It is left capped, to be finished exactly, like any capped record, if the parse comes.
+        v = M_SAT | r;
       } else {
         const uint32_t w = atomicAdd(&nwork, 1u);
         wl[2 * w] = li | (l << 16);
