@@ -1099,9 +1099,65 @@ def run_serve(args):
             pool.append(dict(data=pdata[0], bl=bl, lv=lv, blob=pblob[0], clens=clens, meth=meth.copy(), rlens=rlens,
                              crcs=crcs.copy(), keep=(pdata[1], pblob[1])))
     srv = Z.Server(budget_bytes=args.budget_gib << 30, device=local, pinned=True)
+    plain_codec = Z.CudaCodec(level=5, device=local)
     rates = [float(r) for r in args.rates.split(",")]
     results = []
+
+    def draw_jobs(rate):
+        """The job stream of one rate: (arrival s, pool index, kind u), from the rate's own seed, so that the
+        served and the plain form see the same jobs at the same times."""
+        g = np.random.default_rng(int(rate * 1000) + 17)
+        out, t = [], 0.0
+        while True:
+            t += g.exponential(1.0 / rate)
+            if t > args.duration:
+                return out
+            out.append((t, int(g.integers(len(pool))), float(g.random())))
+
+    def plain_form(jobs):
+        """The plain per-job form: one worker takes the jobs in arrival order and runs each alone through the
+        host-pointer calls (zc_compress; zc_decompress, CRCs compared for a test), as a server without
+        batching would."""
+        q = queue.Queue()
+        lat, nb = [], [0]
+
+        def worker():
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                t_arr, idx, u = item
+                j = pool[idx]
+                if u < 0.6:
+                    plain_codec.compress_arrays(j["data"], j["bl"], level=j["lv"])
+                    nb[0] += j["data"].size
+                else:
+                    coffs = np.concatenate([[0], np.cumsum(j["clens"])[:-1]]).astype(np.uint64)
+                    plain_codec.prepare(j["bl"])
+                    raw, crcs, errs = plain_codec.decompress_arrays(j["blob"], coffs, j["clens"], j["meth"], j["rlens"])
+                    if u >= 0.9:
+                        assert np.array_equal(crcs, j["crcs"])
+                    nb[0] += int(j["rlens"].sum())
+                lat.append(time.perf_counter() - (t0p + t_arr))
+
+        th = threading.Thread(target=worker, daemon=True)
+        t0p = time.perf_counter()
+        th.start()
+        for t_arr, idx, u in jobs:
+            delay = t0p + t_arr - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            q.put((t_arr, idx, u))
+        q.put(None)
+        th.join()
+        wall = time.perf_counter() - t0p
+        lat_ms = np.array(lat) * 1e3
+        return {"achieved_gbs": round(nb[0] / wall / 1e9, 3), "wall_s": round(wall, 2),
+                "p50_ms": round(float(np.percentile(lat_ms, 50)), 2) if len(lat) else None,
+                "p99_ms": round(float(np.percentile(lat_ms, 99)), 2) if len(lat) else None}
+
     for rate in rates:
+        jobs = draw_jobs(rate)
         done_q = queue.Queue()
         lat, nbytes, statuses = [], [0], []
 
@@ -1121,15 +1177,11 @@ def run_serve(args):
         t_next = 0.0
         njobs = 0
         s0 = srv.stats()
-        while True:
-            t_next += rng.exponential(1.0 / rate)
-            if t_next > args.duration:
-                break
+        for t_next, idx, u in jobs:
             delay = t0 + t_next - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            j = pool[int(rng.integers(len(pool)))]
-            u = rng.random()
+            j = pool[idx]
             if u < 0.6:
                 h = srv.compress(j["data"], j["bl"], j["lv"])
                 h.nbytes = j["data"].size
@@ -1154,17 +1206,22 @@ def run_serve(args):
                         "wall_s": round(wall, 2),
                         "gpu_busy": round((s1["gpu_s"] - s0["gpu_s"]) / wall, 3),
                         "worker_s": {k: round(s1[k] - s0[k], 3) for k in ("wait_s", "handout_s", "upload_s")}})
+        if not args.no_plain:
+            results[-1]["plain"] = plain_form(jobs)
         print(json.dumps({"serve_rate": results[-1]}), file=sys.stderr, flush=True)
         if wall > args.duration * 2.0:  # saturated: the backlog took as long again as the arrivals
             break
     srv.close()
+    plain_codec.close()
     best = max(results, key=lambda r: r["achieved_gbs"])
     line = {"metric": METRIC, "value": best["achieved_gbs"], "unit": "GB/s", "n_gpus": 1, "higher_is_better": True,
             "scaling": "weak", "dtype": "u8", "data": "synthetic (seeded per-file generators)",
             "config": {"workload": f"serving: Poisson jobs 60/30/10 compress/extract/test, sizes log-uniform "
                                    f"4 KiB-{args.max_job_mib} MiB (pool of {args.pool} files), block 16/18/20, "
                                    f"level 1/5/9, {args.budget_gib} GiB admission budget, {args.duration} s per rate"},
-            "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "sweep": results}
+            "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "plain_at_that_rate": best.get("plain"),
+            "plain_best_gbs": max((r["plain"]["achieved_gbs"] for r in results if "plain" in r), default=None),
+            "sweep": results}
     print(json.dumps(line), flush=True)
     return 0 if all(r["errors"] == 0 for r in results) else 1
 
@@ -1187,6 +1244,7 @@ def main():
     ap.add_argument("--fill-ring-log", type=int, default=0, help="decode: the fill's ring size (log2 bytes)")
     ap.add_argument("--fill-warps", type=int, default=0, help="decode: the fill's warps per CTA")
     ap.add_argument("--chunk-mib", type=int, default=0, help="batched: encoder launches of at most this many MiB")
+    ap.add_argument("--no-plain", action="store_true", help="serve: skip the plain per-job form beside the server")
     ap.add_argument("--files", type=int, default=10000)
     ap.add_argument("--max-file-kib", type=int, default=1024)
     ap.add_argument("--pool", type=int, default=48, help="serve: distinct files the jobs draw from")

@@ -172,13 +172,20 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_sort_scatter(EncArgs A) {
   if (tid < 256) dst[tid] = A.scnt[((size_t)b * sort_tiles(A.B) + t) * 256 + tid];
   __syncthreads();
   // ranks: warp w holds the tile's entries [kSortPer * 32 w, kSortPer * 32 (w + 1)), 32 per round, in order
+  // (all of a thread's entries are loaded first: the ranking's warp syncs would otherwise keep each load
+  // behind the previous entry's ranking)
   uint32_t kp[kSortPer], kh[kSortPer], kr[kSortPer];
 #pragma unroll
   for (uint32_t j = 0; j < kSortPer; ++j) {
     const uint32_t li = w * (32 * kSortPer) + j * 32 + lane;
+    kp[j] = 0; kh[j] = 0;
+    if (li < tn) sort_load<PASS>(A, b, i0 + li, kp[j], kh[j]);
+  }
+#pragma unroll
+  for (uint32_t j = 0; j < kSortPer; ++j) {
+    const uint32_t li = w * (32 * kSortPer) + j * 32 + lane;
     const bool on = li < tn;
-    uint32_t p = 0, h = 0;
-    if (on) sort_load<PASS>(A, b, i0 + li, p, h);
+    const uint32_t p = kp[j], h = kh[j];
     const uint32_t d = sort_digit<PASS>(h);
     const unsigned act = __ballot_sync(kFull, on);
     uint32_t rk = 0xFFFFFFFFu;
