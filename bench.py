@@ -623,6 +623,10 @@ def run_sweep(args):
                                    else G.random_bytes(n, 77))
             host = data_cache[key]
             codec = Z.CudaCodec(level=lv, device=local)
+            shape = None
+            if args.autotune:  # the cell's launch shape chosen on a sample of its own data (no byte changes)
+                shape = codec.autotune(host[:min(n, args.tune_mib << 20)], bl, lv)
+            codec.prepare(bl)
             per = codec.batch_bytes(bl) // B
             dper = codec.batch_bytes_decode(bl) // B
             d_in = torch.zeros(n + 64, dtype=torch.uint8, device=dev)
@@ -672,7 +676,8 @@ def run_sweep(args):
             comp = int(clens.sum().item())
             cell = {"data": kind, "bytes": n, "block_log": bl, "level": lv, "compress_gbs": round(n / tc / 1e6, 3),
                     "decompress_gbs": round(n / td / 1e6, 3), "round_trip_gbs": round(n / (tc + td) / 1e6, 3),
-                    "ratio": round(comp / n, 5), "stored_blocks": int((methods == 0).sum().item()), "bit_exact": ok}
+                    "ratio": round(comp / n, 5), "stored_blocks": int((methods == 0).sum().item()), "bit_exact": ok,
+                    "shape": shape if shape is not None else codec.get_shape(bl, lv), "autotuned": shape is not None}
             if have_ref:
                 k = min(nb, max(4, (8 << 20) >> bl))
                 rm, rl, rp = O.Ref.cpu_compress(host[:k * B], bl, O.depth_for_level(lv))
@@ -1245,6 +1250,8 @@ def main():
     ap.add_argument("--fill-warps", type=int, default=0, help="decode: the fill's warps per CTA")
     ap.add_argument("--chunk-mib", type=int, default=0, help="batched: encoder launches of at most this many MiB")
     ap.add_argument("--no-plain", action="store_true", help="serve: skip the plain per-job form beside the server")
+    ap.add_argument("--autotune", action="store_true", help="sweep: autotune each cell's launch shape first")
+    ap.add_argument("--tune-mib", type=int, default=128, help="sweep: the autotuner's sample of each cell (MiB)")
     ap.add_argument("--files", type=int, default=10000)
     ap.add_argument("--max-file-kib", type=int, default=1024)
     ap.add_argument("--pool", type=int, default=48, help="serve: distinct files the jobs draw from")

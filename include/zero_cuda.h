@@ -165,7 +165,8 @@ int zc_autotune(zc_ctx *ctx, const uint8_t *sample, size_t n, uint32_t block_log
 
 /* ---- serving: a request loop with continuous batching (no reference counterpart; the reference runs
  * one archive job at a time).  Jobs arrive from any thread; a worker thread admits them in arrival order
- * while their device memory fits in `budget_bytes` (one arena allocated at open), keeps their bytes and
+ * while their device memory fits in the arena (allocated at open: budget_bytes, or less when the device has
+ * less free memory beside the server's own scratch, 1 GiB kept free), keeps their bytes and
  * results on the device, and each tick launches one batch of blocks taken from every admitted job of one
  * kind, block size and level, so jobs that arrive while others run share the launches.  The batches
  * have a fixed capacity (padded with empty blocks) and run as CUDA graphs.
@@ -201,8 +202,10 @@ typedef struct {
 
 typedef struct zc_server zc_server;
 
-/* Opens a server on `device` with a device arena of budget_bytes for the admitted jobs' data (the
- * codec's own scratch comes on top).  max_batch_bytes bounds one tick's input (0: the codec's default). */
+/* Opens a server on `device`.  The codec's scratch for the largest batch of every block size is sized
+ * first; then the arena for the admitted jobs' data: budget_bytes, capped by the device's free memory at
+ * that point less 1 GiB (ZC_E_NOMEM below 1 MiB).  max_batch_bytes bounds one tick's input (0: the codec's
+ * default). */
 int zc_serve_open(zc_server **srv, int device, uint64_t budget_bytes, uint64_t max_batch_bytes);
 /* Waits for every submitted job, then stops the worker and frees the device memory. */
 void zc_serve_close(zc_server *srv);

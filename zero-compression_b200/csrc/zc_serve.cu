@@ -84,6 +84,7 @@ Cls cls_of(const Job* J) {
 }
 
 constexpr uint32_t kCap = 4096;  // blocks per batch at most (padded to a fixed count per block size)
+constexpr uint64_t kFreeMargin = 1ull << 30;  // device memory the arena leaves free
 
 }  // namespace
 
@@ -462,11 +463,6 @@ int zc_serve_open(zc_server** out, int device, uint64_t budget_bytes, uint64_t m
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->ust, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->cst, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMalloc(&S->arena.base, std::max<uint64_t>(budget_bytes, 1u << 20));
-  if (e == cudaSuccess) {
-    S->arena.size = std::max<uint64_t>(budget_bytes, 1u << 20);
-    S->arena.free_[0] = S->arena.size;
-  }
   for (Slot& L : S->slot) {
     if (e == cudaSuccess) e = cudaMalloc(&L.d_a64, kCap * 8 * 3);
     if (e == cudaSuccess) { L.d_b64 = L.d_a64 + kCap; L.d_total = L.d_b64 + kCap; }
@@ -485,6 +481,21 @@ int zc_serve_open(zc_server** out, int device, uint64_t budget_bytes, uint64_t m
   if (e == cudaSuccess) rc = zc_set_graphs(S->ctx, 1);
   // the codec's scratch for the largest batch of every block size, once: ticks then never reallocate it
   for (uint32_t bl = 16; bl <= 20 && e == cudaSuccess && !rc; ++bl) rc = zc_reserve(S->ctx, bl, batch_cap(S, bl));
+  // the jobs' arena, last: the budget, but no more than the device has free now beside everything above
+  // (less kFreeMargin for the runtime and other users), so that admission against it is admission by the
+  // device's free memory
+  if (e == cudaSuccess && !rc) {
+    size_t free_b = 0, total_b = 0;
+    e = cudaMemGetInfo(&free_b, &total_b);
+    const uint64_t room = free_b > kFreeMargin ? free_b - kFreeMargin : 0;
+    const uint64_t size = std::min<uint64_t>(std::max<uint64_t>(budget_bytes, 1u << 20), room);
+    if (e == cudaSuccess && size < (1u << 20)) e = cudaErrorMemoryAllocation;
+    if (e == cudaSuccess) e = cudaMalloc(&S->arena.base, size);
+    if (e == cudaSuccess) {
+      S->arena.size = size;
+      S->arena.free_[0] = size;
+    }
+  }
   if (e != cudaSuccess || rc) {
     zc_serve_close(S);
     return e == cudaErrorMemoryAllocation ? ZC_E_NOMEM : (rc ? rc : ZC_E_DEVICE);
