@@ -9,8 +9,9 @@
 //                  CTA per 4096-position tile: digit counts, per-block scan, ranked scatter (warp
 //                  match_any ranks, the tile reordered in shared memory, digit runs written together)
 //   k_enc_match    per sorted position (lanes take positions from a per-CTA counter): scans its chain,
-//                  comparing at most cmp_cap bytes; a match that reaches cmp_cap is marked and finished
-//                  only if the parse visits it
+//                  comparing at most cmp_cap bytes; a match that reaches cmp_cap, or a position that lies
+//                  inside a longer match starting before it, is marked and finished only if the parse
+//                  visits it
 //   k_enc_parse    one CTA per block: the greedy + lazy parse as a chain 0 -> next(0) -> ..., walked
 //                  per segment in parallel from the segment start, then re-walked from the true entry
 //                  until it meets the first walk (rounds until no segment exit moves); a warp's walks
