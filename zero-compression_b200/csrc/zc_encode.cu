@@ -8,10 +8,11 @@
 //   k_sort_*       stable two-pass LSD radix sort of each block's positions by hash (8 + 8 bits), a
 //                  CTA per 4096-position tile: digit counts, per-block scan, ranked scatter (warp
 //                  match_any ranks, the tile reordered in shared memory, digit runs written together)
-//   k_enc_match    per sorted position (lanes take positions from a per-CTA counter): scans its chain,
-//                  comparing at most cmp_cap bytes; a match that reaches cmp_cap, or a position that lies
-//                  inside a longer match starting before it, is marked and finished only if the parse
-//                  visits it
+//   k_enc_match    per sorted position: its nearest candidate, then, where that does not decide it, its
+//                  chain scanned (by a lane, or by a group of lanes a candidate each where the tile has few
+//                  such positions), comparing at most cmp_cap bytes; a match that reaches cmp_cap, or a
+//                  position that lies inside a longer match starting before it, is marked and finished
+//                  only if the parse visits it
 //   k_enc_parse    one CTA per block: the greedy + lazy parse as a chain 0 -> next(0) -> ..., walked
 //                  per segment in parallel from the segment start, then re-walked from the true entry
 //                  until it meets the first walk (rounds until no segment exit moves); a warp's walks
@@ -268,14 +269,23 @@ __device__ __forceinline__ uint32_t lcp32(const uint4& a0, const uint4& a1, cons
   return 32;
 }
 
+#ifndef ZC_MATCH_GROUP
+#define ZC_MATCH_GROUP 16
+#endif
+constexpr uint32_t kMatchGroup = ZC_MATCH_GROUP;  // lanes per work-list entry in the match pass: 8, 16 or 32
+#ifndef ZC_MATCH_DENSE
+#define ZC_MATCH_DENSE 256
+#endif
+constexpr uint32_t kMatchDense = ZC_MATCH_DENSE;  // work-list entries from which a tile scans a lane per entry
+static_assert(kMatchGroup == 8 || kMatchGroup == 16 || kMatchGroup == 32, "lanes per work-list entry");
+
 // One CTA of 256 threads per `tile` consecutive sorted positions of a block (tile = A.match_tile, a
 // multiple of 256).  The entries it needs (its own and the `depth` before them) are staged once in
 // shared memory with the first WB bytes at each position (WB = 16 or 32, at least the compare cap), so
-// a candidate costs a few shared loads and XORs instead of random global reads.  Chains differ in length, so lanes do not own fixed positions:
-// each lane takes the CTA's next unscanned position from a shared counter whenever its own is finished
-// (a warp claims positions for all its idle lanes at once), keeping warps full until the tile drains.
-// A candidate whose byte at the current best length differs from the position's cannot be longer and
-// is skipped after one shared byte load (the CPU parse's probe, src/codec2.h:62).
+// a candidate costs a few shared loads and XORs instead of random global reads.  Pass 1 gives each
+// position its nearest candidate, which decides most of them; the rest go to a work list, scanned a lane
+// per entry when it fills the CTA's lanes (or chains are short), else by groups of lanes, one candidate
+// a lane (one lane per entry would leave most lanes idle while a warp's longest chain finishes).
 // Dynamic shared memory: (tile + depth) * (WB + 4 + 2) + 8 * tile bytes (+4).
 template <uint32_t WB>
 __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
@@ -295,7 +305,6 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   uint32_t* spos = reinterpret_cast<uint32_t*>(win + NV * cap_e);
   uint16_t* sh = reinterpret_cast<uint16_t*>(spos + cap_e);
   uint32_t* wl = reinterpret_cast<uint32_t*>(sh + ((cap_e + 1) & ~1u));  // work list: entry | best << 16, distance
-  const uint8_t* wb = reinterpret_cast<const uint8_t*>(win);
   const uint32_t e0 = r0 > D ? r0 - D : 0, e1 = min(r0 + tile, count);
   const uint64_t base = A.in_off[b];
   // (a window may reach up to WB + 15 bytes past its position, inside the input's readable slack; bytes past
@@ -364,78 +373,116 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   }
   __syncthreads();
   const uint32_t tw = nwork;
-  // pass 2 over the work list, lanes taking entries from a CTA counter.  Per-lane state: the position's
-  // entry li, its chain of kend earlier entries with the same hash (found by a binary search: the
-  // entries are sorted by hash), the candidate k reached so far, the best length, its distance, and the
-  // position's own byte at offset `best` (the probe)
-  uint32_t li = 0xFFFFFFFFu, p = 0, lim = 0, cap = 0, best = 0, bd = 0, k = 0, kend = 0, pb = 0;
-  uint4 p0 = make_uint4(0, 0, 0, 0), p1 = p0;
-  bool dry = false;  // the tile has no unclaimed positions left (warp-uniform)
-  for (;;) {
-    const bool idle = li == 0xFFFFFFFFu;
-    const unsigned want = __ballot_sync(kFull, idle);
-    if (want && !dry) {
-      const uint32_t leader = (uint32_t)__ffs(want) - 1u;
-      uint32_t got = 0;
-      if (lane == leader) got = atomicAdd(&next, (uint32_t)__popc(want));
-      got = __shfl_sync(kFull, got, leader);
-      if (got + (uint32_t)__popc(want) >= tw) dry = true;
-      if (idle) {
-        const uint32_t my = got + (uint32_t)__popc(want & ((1u << lane) - 1u));
-        if (my < tw) {
-          const uint32_t wa = wl[2 * my];
-          li = wa & 0xFFFFu;
-          best = wa >> 16;
-          bd = wl[2 * my + 1];
-          const uint32_t r = li + e0;
-          p = spos[li];
-          const uint32_t h = sh[li];
-          lim = min(kMaxMatch, n - p);
-          cap = min(min(A.cmp_cap, WB), lim);
-          p0 = win[NV * li];
-          p1 = win[NV * li + NV - 1];
-          k = 1;
-          pb = wb[WB * li + best];
-          uint32_t lo = li - min(D, r), hi = li;  // the first entry of [lo, li] with hash h
-          while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (sh[mid] < h) lo = mid + 1; else hi = mid;
+  if (tw >= kMatchDense || D <= 8) {
+    // pass 2, a lane per work-list entry (a work list that fills the CTA, or chains of at most 8): lanes take
+    // entries from a CTA counter, a warp claiming entries for all its idle lanes at once.  Per-lane state: the
+    // position's entry li, its chain of kend earlier entries with the same hash (a binary search: the entries
+    // are sorted by hash), the candidate k reached so far, the best length, its distance, and the position's
+    // own byte at offset `best`: a candidate whose byte there differs cannot be longer and is skipped after
+    // one shared byte load (the CPU parse's probe, src/codec2.h:62)
+    const uint8_t* wb = reinterpret_cast<const uint8_t*>(win);
+    uint32_t li = 0xFFFFFFFFu, p = 0, lim = 0, cap = 0, best = 0, bd = 0, k = 0, kend = 0, pb = 0;
+    uint4 p0 = make_uint4(0, 0, 0, 0), p1 = p0;
+    bool dry = false;  // the tile has no unclaimed entries left (warp-uniform)
+    for (;;) {
+      const bool idle = li == 0xFFFFFFFFu;
+      const unsigned want = __ballot_sync(kFull, idle);
+      if (want && !dry) {
+        const uint32_t leader = (uint32_t)__ffs(want) - 1u;
+        uint32_t got = 0;
+        if (lane == leader) got = atomicAdd(&next, (uint32_t)__popc(want));
+        got = __shfl_sync(kFull, got, leader);
+        if (got + (uint32_t)__popc(want) >= tw) dry = true;
+        if (idle) {
+          const uint32_t my = got + (uint32_t)__popc(want & ((1u << lane) - 1u));
+          if (my < tw) {
+            const uint32_t wa = wl[2 * my];
+            li = wa & 0xFFFFu;
+            best = wa >> 16;
+            bd = wl[2 * my + 1];
+            const uint32_t r = li + e0;
+            p = spos[li];
+            const uint32_t h = sh[li];
+            lim = min(kMaxMatch, n - p);
+            cap = min(min(A.cmp_cap, WB), lim);
+            p0 = win[NV * li];
+            p1 = win[NV * li + NV - 1];
+            k = 1;
+            pb = wb[WB * li + best];
+            uint32_t lo = li - min(D, r), hi = li;  // the first entry of [lo, li] with hash h
+            while (lo < hi) {
+              const uint32_t mid = (lo + hi) >> 1;
+              if (sh[mid] < h) lo = mid + 1; else hi = mid;
+            }
+            kend = li - lo;
           }
-          kend = li - lo;
         }
       }
-    }
-    if (!__any_sync(kFull, li != 0xFFFFFFFFu)) break;
-    if (li == 0xFFFFFFFFu) continue;
-    // four candidates of this lane's chain: probes first, full compares for those that pass, in order
-    bool fin = false;
-    uint32_t pass = 0;
+      if (!__any_sync(kFull, li != 0xFFFFFFFFu)) break;
+      if (li == 0xFFFFFFFFu) continue;
+      // four candidates of this lane's chain: probes first, full compares for those that pass, in order
+      bool fin = false;
+      uint32_t pass = 0;
 #pragma unroll
-    for (uint32_t u = 0; u < 4; ++u) {
-      const uint32_t kk = k + 1 + u;
-      if (kk <= kend && (best == 0 || wb[WB * (li - kk) + best] == pb)) pass |= 1u << u;
-    }
-    while (pass) {
-      const uint32_t u = (uint32_t)__ffs(pass) - 1u;
-      pass &= pass - 1u;
-      const uint32_t kk = k + 1 + u, e = li - kk;
-      const uint32_t l = min(NV == 2 ? lcp32(win[2 * e], win[2 * e + 1], p0, p1) : lcp16(win[e], p0), cap);
-      if (l > best) {
-        best = l;
-        bd = p - spos[e];
-        if (best == cap) { fin = true; break; }
-        pb = wb[WB * li + best];
+      for (uint32_t u = 0; u < 4; ++u) {
+        const uint32_t kk = k + 1 + u;
+        if (kk <= kend && (best == 0 || wb[WB * (li - kk) + best] == pb)) pass |= 1u << u;
+      }
+      while (pass) {
+        const uint32_t u = (uint32_t)__ffs(pass) - 1u;
+        pass &= pass - 1u;
+        const uint32_t kk = k + 1 + u, e = li - kk;
+        const uint32_t l = min(NV == 2 ? lcp32(win[2 * e], win[2 * e + 1], p0, p1) : lcp16(win[e], p0), cap);
+        if (l > best) {
+          best = l;
+          bd = p - spos[e];
+          if (best == cap) { fin = true; break; }
+          pb = wb[WB * li + best];
+        }
+      }
+      k += 4;
+      if (fin || k >= kend) {
+        A.minfo[so + p] = best < 4 ? M_NONE : best == cap && cap < lim ? M_SAT | (li + e0) : m_pack(best, bd);
+        li = 0xFFFFFFFFu;
       }
     }
-    k += 4;
-    if (fin || k >= kend) {
-      uint32_t v;
-      if (best < 4) v = M_NONE;
-      else if (best == cap && cap < lim) v = M_SAT | (li + e0);
-      else v = m_pack(best, bd);
-      A.minfo[so + p] = v;
-      li = 0xFFFFFFFFu;
+    return;
+  }
+  // pass 2, kMatchGroup lanes per work-list entry (a short work list: a lane each would leave most lanes
+  // idle while the longest chain finishes): lane g of the group compares the chain's candidate k = kb + g
+  // (kb = 2, then kMatchGroup further each round; candidate 1 was pass 1's), all from shared memory; the
+  // group's longest, the nearest on a tie, replaces the best only when longer, so nearer rounds win ties
+  // too, as in the CPU parse's nearest-first scan.  The chain is the run of entries before the position with
+  // its hash (the entries are sorted by hash), so it ends at the first lane whose entry differs; a round
+  // ends the scan when the chain ends in it or the best reaches the cap.
+  constexpr uint32_t G = kMatchGroup, NG = 32 / G;
+  const uint32_t gl = lane % G;
+  const unsigned gmask = G == 32 ? kFull : ((1u << G) - 1u) << (lane - gl);
+  for (uint32_t wi = (t >> 5) * NG + lane / G; wi < tw; wi += 8 * NG) {
+    const uint32_t wa = wl[2 * wi];
+    const uint32_t li = wa & 0xFFFFu, r = li + e0;
+    uint32_t best = wa >> 16, bd = wl[2 * wi + 1];
+    const uint32_t p = spos[li], h = sh[li];
+    const uint32_t lim = min(kMaxMatch, n - p), cap = min(min(A.cmp_cap, WB), lim);
+    const uint4 p0 = win[NV * li], p1 = win[NV * li + NV - 1];
+    const uint32_t kmax = min(D, r);  // (li >= kmax: the tile's entries are staged from depth before it)
+    for (uint32_t kb = 2; kb <= kmax; kb += G) {
+      const uint32_t k = kb + gl;
+      const bool on = k <= kmax && sh[li - k] == h;
+      uint32_t key = 0;
+      if (on) {
+        const uint32_t e = li - k;
+        const uint32_t l = min(NV == 2 ? lcp32(win[2 * e], win[2 * e + 1], p0, p1) : lcp16(win[e], p0), cap);
+        key = (l << 8) | (G - 1u - gl);  // (l <= 32)
+      }
+      const uint32_t mk = __reduce_max_sync(gmask, key);
+      if ((mk >> 8) > best) {
+        best = mk >> 8;
+        bd = p - spos[li - (kb + G - 1u - (mk & 0xFFu))];
+      }
+      if (best == cap || __ballot_sync(gmask, on) != gmask) break;
     }
+    if (gl == 0) A.minfo[so + p] = best < 4 ? M_NONE : best == cap && cap < lim ? M_SAT | r : m_pack(best, bd);
   }
 }
 
