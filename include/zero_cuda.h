@@ -153,11 +153,14 @@ int zc_reserve(zc_ctx *ctx, uint32_t block_log, uint32_t nb);
  *   match_tile      encoder match pass: sorted positions per CTA of 256 threads (256, 512 or 1024)
  *   fill_words      decoder fill: output words each lane fills per round (1, 2 or 4: rounds of 128,
  *                   256 or 512 bytes, whose loads are in flight together)
+ *   match_dense     encoder match pass: a tile with at least this many positions that their nearest
+ *                   candidate does not decide scans a lane per position, a tile with fewer a 16-lane group
+ *                   per position, a candidate a lane (0..1025; 1025: always groups, except at level 1)
  * The decoder uses the shape of the level last given to zc_prepare (5 by default).  zc_autotune times
  * the candidates on a host sample (its whole blocks, up to one encoder launch) and keeps the fastest for
  * (block_log, level); it allocates its own device buffers for the duration of the call. */
 typedef struct zc_shape {
-  uint32_t fill_ring_log, fill_warps, match_cap, match_tile, fill_words;
+  uint32_t fill_ring_log, fill_warps, match_cap, match_tile, fill_words, match_dense;
 } zc_shape;
 int zc_get_shape(const zc_ctx *ctx, uint32_t block_log, int level, zc_shape *out);
 int zc_set_shape(zc_ctx *ctx, uint32_t block_log, int level, const zc_shape *shape);

@@ -36,7 +36,9 @@ namespace zc {
 // top 12 bits, and r < 2^20 - 3, so SAT | r is never NONE.
 constexpr uint32_t M_NONE = 0xFFFFFFFFu;
 constexpr uint32_t M_SAT = 0xFFF00000u;
-__device__ __forceinline__ bool m_is_sat(uint32_t v) { return (v >> 20) == 0xFFFu && v != M_NONE; }
+constexpr uint32_t M_BELOW = 0xFFE00000u;  // capped, and known to lose the lazy test of the position before
+__device__ __forceinline__ bool m_is_sat(uint32_t v) { return (v >> 20) >= 0xFFEu && v != M_NONE; }
+__device__ __forceinline__ bool m_is_below(uint32_t v) { return (v >> 20) == 0xFFEu; }
 __device__ __forceinline__ uint32_t m_pack(uint32_t m, uint32_t d) { return ((m - 4u) << 20) | (d - 1u); }
 __device__ __forceinline__ uint32_t m_len(uint32_t v) { return (v >> 20) + 4u; }
 __device__ __forceinline__ uint32_t m_dist(uint32_t v) { return (v & 0xFFFFFu) + 1u; }
@@ -273,10 +275,6 @@ __device__ __forceinline__ uint32_t lcp32(const uint4& a0, const uint4& a1, cons
 #define ZC_MATCH_GROUP 16
 #endif
 constexpr uint32_t kMatchGroup = ZC_MATCH_GROUP;  // lanes per work-list entry in the match pass: 8, 16 or 32
-#ifndef ZC_MATCH_DENSE
-#define ZC_MATCH_DENSE 256
-#endif
-constexpr uint32_t kMatchDense = ZC_MATCH_DENSE;  // work-list entries from which a tile scans a lane per entry
 static_assert(kMatchGroup == 8 || kMatchGroup == 16 || kMatchGroup == 32, "lanes per work-list entry");
 
 // One CTA of 256 threads per `tile` consecutive sorted positions of a block (tile = A.match_tile, a
@@ -373,7 +371,7 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   }
   __syncthreads();
   const uint32_t tw = nwork;
-  if (tw >= kMatchDense || D <= 8) {
+  if (tw >= A.match_dense || D <= 8) {
     // pass 2, a lane per work-list entry (a work list that fills the CTA, or chains of at most 8): lanes take
     // entries from a CTA counter, a warp claiming entries for all its idle lanes at once.  Per-lane state: the
     // position's entry li, its chain of kend earlier entries with the same hash (a binary search: the entries
@@ -503,12 +501,16 @@ struct ParseBlock {
 // are extended in chain order by the whole warp, 128 bytes a step.  The longest wins, the nearest on a
 // tie, and a match of the whole remaining length ends the walk, as in the CPU parse.  The exact record
 // replaces the capped one in minfo.
-__device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x) {
+// With need > 0 the caller only needs the exact match if it is at least `need` bytes long: a candidate whose
+// byte at need - 1 differs from x's is shorter and dropped after that one load, and when no candidate
+// reaches need the result is NONE and minfo keeps the capped record.
+__device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x, uint32_t need = 0) {
   const uint32_t lane = lane_id();
   const uint32_t v = P.minfo[x];
   if (!m_is_sat(v)) return v;
   const uint32_t r = v & 0xFFFFFu, h = P.sh[r];
   const uint32_t lim = min(kMaxMatch, P.n - x);
+  if (need > lim) return M_NONE;
   const uint32_t l32 = min(32u, lim);
   const uint32_t kmax = min(P.depth, r);
   const uint64_t ax = P.base + x;
@@ -520,8 +522,9 @@ __device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x) {
     const unsigned chain = __ballot_sync(kFull, in_chain);
     const unsigned live = ~chain ? chain & ((1u << __ffs(~chain) - 1) - 1u) : chain;  // up to the first break
     if (live != chain || chain != kFull) stop = true;  // the chain ends in this chunk
-    const bool on = (live >> lane) & 1u;
+    bool on = (live >> lane) & 1u;
     const uint32_t j = on ? P.spos[r - k] : 0u;
+    if (need && on) on = __ldg(P.in + P.base + j + need - 1) == __ldg(P.in + ax + need - 1);
     uint32_t l = 0;
     if (on) {  // 16 bytes a round from independent word loads (at most two rounds)
       const uint64_t aj = P.base + j;
@@ -573,6 +576,12 @@ __device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x) {
       }
     }
   }
+  if (best < need) {  // (warp-uniform) marked, so a later walk's lazy test skips it
+    __syncwarp();
+    if (lane == 0) P.minfo[x] = M_BELOW | r;
+    __syncwarp();
+    return M_NONE;
+  }
   const uint32_t e = m_pack(best, bd);
   __syncwarp();
   if (lane == 0) P.minfo[x] = e;
@@ -597,11 +606,15 @@ __device__ __forceinline__ uint32_t warp_step(const ParseBlock& P, uint32_t p, u
     const uint32_t e = coop_exact(P, __shfl_sync(kFull, p, L));
     if (lane_id() == L) v = e;
   }
+  // the match at p + 1 replaces p's only if 8 m2 - bitlen(d2) - 8 > 8 m - bitlen(d), so (bitlen(d2) >= 0)
+  // only if 8 m2 > 8 m + 8 - bitlen(d), m2 >= need; a shorter one is never needed exactly
+  const uint32_t need = lz ? ((8u * m_len(v) + 8u - bitlen(m_dist(v))) >> 3) + 1u : 0u;
+  if (m_is_below(v2)) v2 = M_NONE;
   unsigned s2 = __ballot_sync(kFull, lz && m_is_sat(v2));
   while (s2) {
     const uint32_t L = (uint32_t)__ffs(s2) - 1u;
     s2 &= s2 - 1u;
-    const uint32_t e = coop_exact(P, __shfl_sync(kFull, p, L) + 1u);
+    const uint32_t e = coop_exact(P, __shfl_sync(kFull, p, L) + 1u, __shfl_sync(kFull, need, L));
     if (lane_id() == L) v2 = e;
   }
   tok = false;
