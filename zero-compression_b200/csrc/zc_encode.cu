@@ -31,9 +31,11 @@ namespace zc {
 
 // per-position match record: NONE; SAT | r (a candidate reached cmp_cap, or the position lies inside a
 // longer match that starts before it; r is the position's index in the hash-sorted order, where its chain
-// starts: finished on demand by the parse, which computes the chain's exact best); or the exact
-// (length - 4) << 20 | (distance - 1).  Lengths are <= 4096, so an exact record never has 0xFFF in its
-// top 12 bits, and r < 2^20 - 3, so SAT | r is never NONE.
+// starts: finished on demand by the parse, which computes the chain's exact best); BELOW | r (the parse
+// found that the position's match cannot win the lazy test of the position before it, and left it
+// unfinished: finished like SAT if a walk needs it exactly); or the exact (length - 4) << 20 |
+// (distance - 1).  Lengths are <= 4096, so an exact record has at most 0xFFC in its top 12 bits, and
+// r < 2^20 - 3, so SAT | r is never NONE.
 constexpr uint32_t M_NONE = 0xFFFFFFFFu;
 constexpr uint32_t M_SAT = 0xFFF00000u;
 constexpr uint32_t M_BELOW = 0xFFE00000u;  // capped, and known to lose the lazy test of the position before
@@ -549,11 +551,15 @@ __device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x, uint32_t need = 
     // candidates equal for 32 bytes: extended in chain order
     unsigned ext = __ballot_sync(kFull, on && l == 32u && lim > 32u);
     while (ext) {
+      // (best >= 32 < lim here) a candidate whose byte at `best` differs from x's is no longer than best:
+      // all such are dropped at once, before the next one in chain order is extended
+      const bool keep = ((ext >> lane) & 1u) && __ldg(P.in + P.base + j + best) == __ldg(P.in + ax + best);
+      ext = __ballot_sync(kFull, keep);
+      if (!ext) break;
       const uint32_t c = (uint32_t)__ffs(ext) - 1u;
       ext &= ext - 1u;
       const uint32_t jc = __shfl_sync(kFull, j, c);
       const uint64_t aj = P.base + jc;
-      if (best > 32 && __ldg(P.in + aj + min(best, lim - 1)) != __ldg(P.in + ax + min(best, lim - 1))) continue;
       uint32_t len = lim;
       for (uint32_t o = 32; o < lim; o += 128) {
         const uint32_t q = o + 4 * lane;
@@ -582,7 +588,7 @@ __device__ uint32_t coop_exact(const ParseBlock& P, uint32_t x, uint32_t need = 
     __syncwarp();
     return M_NONE;
   }
-  const uint32_t e = m_pack(best, bd);
+  const uint32_t e = best < 4 ? M_NONE : m_pack(best, bd);  // (capped records match >= 4 bytes: never NONE)
   __syncwarp();
   if (lane == 0) P.minfo[x] = e;
   __syncwarp();
