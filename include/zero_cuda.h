@@ -156,11 +156,15 @@ int zc_reserve(zc_ctx *ctx, uint32_t block_log, uint32_t nb);
  *   match_dense     encoder match pass: a tile with at least this many positions that their nearest
  *                   candidate does not decide scans a lane per position, a tile with fewer a 16-lane group
  *                   per position, a candidate a lane (0..1025; 1025: always groups, except at level 1)
+ *   match_defer     encoder match pass: a position whose nearest candidate's match also covers the
+ *                   match_defer bytes before it lies inside a longer match and is left to the parse to
+ *                   finish only if it lands there (0..4; 0: never; 2 by default, more for text-like data
+ *                   whose parse lands on such positions more often)
  * The decoder uses the shape of the level last given to zc_prepare (5 by default).  zc_autotune times
  * the candidates on a host sample (its whole blocks, up to one encoder launch) and keeps the fastest for
  * (block_log, level); it allocates its own device buffers for the duration of the call. */
 typedef struct zc_shape {
-  uint32_t fill_ring_log, fill_warps, match_cap, match_tile, fill_words, match_dense;
+  uint32_t fill_ring_log, fill_warps, match_cap, match_tile, fill_words, match_dense, match_defer;
 } zc_shape;
 int zc_get_shape(const zc_ctx *ctx, uint32_t block_log, int level, zc_shape *out);
 int zc_set_shape(zc_ctx *ctx, uint32_t block_log, int level, const zc_shape *shape);

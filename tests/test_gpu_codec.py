@@ -228,7 +228,7 @@ def test_graph_replay_matches_direct(codec):
 
 def test_launch_shapes_never_change_bytes(codec):
     """Every decoder fill shape (ring size, warps per CTA, words per lane) and encoder match shape (cap, tile,
-    lane-or-group threshold) gives the same bytes; the autotuner's choice too.  Data with near and far
+    lane-or-group threshold, deferral length) gives the same bytes; the autotuner's choice too.  Data with near and far
     matches, long runs and stored blocks."""
     import datagen as G
     default = {bl: codec.get_shape(bl, 5) for bl in (16, 18)}
@@ -240,14 +240,14 @@ def test_launch_shapes_never_change_bytes(codec):
             ref = cpu_blocks(data.tobytes(), bl, 5)
             ref_m = [m for m, _ in ref]
             ref_p = [p for _, p in ref]
-            for cap, tile, dense in ((8, 256, 256), (12, 1024, 0), (20, 512, 1025), (32, 256, 64), (32, 1024, 1025),
-                                     (16, 1024, 0), (16, 1024, 1025)):
-                codec.set_shape(bl, 5, match_cap=cap, match_tile=tile, match_dense=dense)
+            for cap, tile, dense, defer in ((8, 256, 256, 2), (12, 1024, 0, 0), (20, 512, 1025, 3), (32, 256, 64, 4),
+                                            (32, 1024, 1025, 1), (16, 1024, 0, 4), (16, 1024, 1025, 0)):
+                codec.set_shape(bl, 5, match_cap=cap, match_tile=tile, match_dense=dense, match_defer=defer)
                 meth, lens, crcs, pay, offs = codec.compress_arrays(data, bl, level=5)
-                assert list(meth) == ref_m, (cap, tile, dense)
+                assert list(meth) == ref_m, (cap, tile, dense, defer)
                 for b, p in enumerate(ref_p):
                     if p is not None:
-                        assert pay[int(offs[b]): int(offs[b]) + int(lens[b])].tobytes() == p, (cap, tile, dense, b)
+                        assert pay[int(offs[b]): int(offs[b]) + int(lens[b])].tobytes() == p, (cap, tile, dense, defer, b)
             codec.prepare(bl)
             raw_lens = [min(B, data.size - o) for o in range(0, data.size, B)]
             comp = [p if p is not None else data[o:o + B].tobytes() for p, o in zip(ref_p, range(0, data.size, B))]

@@ -192,6 +192,7 @@ int encode_device(zc_ctx* c, const uint8_t* d_in, const uint64_t* d_off, const u
   A.cmp_cap = sh.cmp_cap;
   A.match_tile = sh.match_tile;
   A.match_dense = sh.match_dense;
+  A.match_defer = sh.match_defer;
   A.tmp_pos = c->e_tmp_pos.as<uint32_t>(); A.srt_pos = c->e_srt_pos.as<uint32_t>();
   A.minfo = c->e_minfo.as<uint32_t>(); A.scnt = c->e_scnt.as<uint32_t>();
   A.tk_seg = c->e_tk_seg.as<uint32_t>();
@@ -592,6 +593,7 @@ int zc_get_shape(const zc_ctx* c, uint32_t block_log, int level, zc_shape* out) 
   out->match_tile = s.match_tile;
   out->fill_words = s.fill_words;
   out->match_dense = s.match_dense;
+  out->match_defer = s.match_defer;
   return ZC_OK;
 }
 
@@ -603,7 +605,7 @@ int zc_set_shape(zc_ctx* c, uint32_t block_log, int level, const zc_shape* in) {
       (w != 1 && w != 2 && w != 4 && w != 8) || in->match_cap < 8 ||
       (in->fill_words != 1 && in->fill_words != 2 && in->fill_words != 4) ||
       in->match_cap > 32 || zc::fill_smem_bytes(in->fill_ring_log, w, in->fill_words) > zc::kMaxFillSmem ||
-      (in->match_tile != 256 && in->match_tile != 512 && in->match_tile != 1024) || in->match_dense > 1025)
+      (in->match_tile != 256 && in->match_tile != 512 && in->match_tile != 1024) || in->match_dense > 1025 || in->match_defer > 4)
     return fail(c, ZC_E_ARG, "launch shape out of range");
   ZC_CUDA(cudaSetDevice(c->device));
   Shape& s = c->shape[block_log - zc::kMinBlockLog][level_class(level)];
@@ -613,6 +615,7 @@ int zc_set_shape(zc_ctx* c, uint32_t block_log, int level, const zc_shape* in) {
   s.match_tile = in->match_tile;
   s.fill_words = in->fill_words;
   s.match_dense = in->match_dense;
+  s.match_defer = in->match_defer;
   drop_graphs(c);  // (captured launches carry the old shape)
   return ZC_OK;
 }
@@ -711,6 +714,14 @@ int zc_autotune(zc_ctx* c, const uint8_t* sample, size_t n, uint32_t block_log, 
       float ms;
       if ((r = timed(encode, ms))) break;
       if (ms < best_ms) { best_ms = ms; best.match_dense = dense; }
+    }
+    for (uint32_t back : {2u, 3u, 4u}) {  // (the match pass's savings against the parse's extra finishes)
+      if (r || back == best.match_defer) continue;
+      cur = best;
+      cur.match_defer = back;
+      float ms;
+      if ((r = timed(encode, ms))) break;
+      if (ms < best_ms) { best_ms = ms; best.match_defer = back; }
     }
     if (r) break;
     cur = best;

@@ -241,14 +241,10 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_sort_scatter(EncArgs A) {
 }
 
 // ---------------------------------------------------------------- 2. capped matches at every position
-// A position whose nearest candidate matches at least 4 bytes and also the kDeferBack bytes before them is
-// inside a longer match; the match pass leaves it to the parse (1..4 bytes; the mask selects them in the
-// little-endian word of the 4 bytes before the position)
-#ifndef ZC_DEFER_BACK
-#define ZC_DEFER_BACK 3
-#endif
-constexpr uint32_t kDeferBack = ZC_DEFER_BACK;
-constexpr uint32_t kDeferBackMask = 0xFFFFFFFFu << (8u * (4u - kDeferBack));
+// A position whose nearest candidate matches at least 4 bytes and also the A.match_defer bytes before them
+// (1..4; 0: never) is inside a longer match; the match pass leaves it to the parse.  The mask selects those
+// bytes in the little-endian word of the 4 bytes before the position.
+__device__ __forceinline__ uint32_t defer_mask(uint32_t back) { return back ? 0xFFFFFFFFu << (8u * (4u - back)) : 0u; }
 
 // the first differing byte of two 16-byte windows (16 when equal)
 __device__ __forceinline__ uint32_t lcp16(const uint4& a0, const uint4& b0) {
@@ -301,6 +297,7 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
   const size_t so = (size_t)b * A.B;
   const uint32_t D = (uint32_t)A.depth;
   const uint32_t cap_e = tile + D;
+  const uint32_t dmask = defer_mask(A.match_defer);
   uint4* win = sm;  // entry i: bytes 16 v .. 16 v + 15 at win[NV i + v]
   uint32_t* spos = reinterpret_cast<uint32_t*>(win + NV * cap_e);
   uint16_t* sh = reinterpret_cast<uint16_t*>(spos + cap_e);
@@ -356,9 +353,9 @@ __global__ void __launch_bounds__(256) k_enc_match(EncArgs A) {
         v = cap < lim ? M_SAT | r : m_pack(l, d);
       } else if (r < 2 || D < 2 || sh[li - 2] != h) {
         v = l < 4 ? M_NONE : m_pack(l, d);
-      } else if (l >= 4 && p >= 4 && p - d >= 4 &&
-                 ((load4(A.in, base + p - 4) ^ load4(A.in, base + p - d - 4)) & kDeferBackMask) == 0) {
-        // the nearest candidate's match also runs kDeferBack bytes back, so p lies inside a longer match
+      } else if (dmask && l >= 4 && p >= 4 && p - d >= 4 &&
+                 ((load4(A.in, base + p - 4) ^ load4(A.in, base + p - d - 4)) & dmask) == 0) {
+        // the nearest candidate's match also runs match_defer bytes back, so p lies inside a longer match
         // that starts earlier: the parse rarely visits it (it lands on match starts and the position after
         // them).  It is left capped, to be finished exactly, like any capped record, if the parse comes.
         v = M_SAT | r;

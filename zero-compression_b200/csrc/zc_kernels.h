@@ -77,6 +77,7 @@ struct EncArgs {
   uint32_t cmp_cap;           // bytes the all-position match pass compares before deferring to the parse
   uint32_t match_tile;        // sorted positions per match CTA: 256, 512 or 1024
   uint32_t match_dense;       // unfinished positions from which a match tile scans a lane per position
+  uint32_t match_defer;       // backward bytes that mark a position as inside a longer match (0: none)
   // scratch, per block slot (capacity B positions)
   uint32_t *tmp_pos, *srt_pos, *minfo;
   uint32_t* scnt;                 // sort: per block ceil(B / 4096) * 256 tile digit counts / starts

@@ -110,7 +110,8 @@ def lib():
 class Shape(C.Structure):
     """zc_shape: launch shapes kept per (block_log, level class); none of them changes a result byte."""
     _fields_ = [("fill_ring_log", C.c_uint32), ("fill_warps", C.c_uint32), ("match_cap", C.c_uint32),
-                ("match_tile", C.c_uint32), ("fill_words", C.c_uint32), ("match_dense", C.c_uint32)]
+                ("match_tile", C.c_uint32), ("fill_words", C.c_uint32), ("match_dense", C.c_uint32),
+                ("match_defer", C.c_uint32)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
