@@ -158,8 +158,8 @@ int zc_reserve(zc_ctx *ctx, uint32_t block_log, uint32_t nb);
  *                   per position, a candidate a lane (0..1025; 1025: always groups, except at level 1)
  *   match_defer     encoder match pass: a position whose nearest candidate's match also covers the
  *                   match_defer bytes before it lies inside a longer match and is left to the parse to
- *                   finish only if it lands there (0..4; 0: never; 2 by default, more for text-like data
- *                   whose parse lands on such positions more often)
+ *                   finish only if it lands there (0..4; 0: never; 3 by default: 2 is faster on data
+ *                   with long matches, 3-4 on text-like data whose parse lands on such positions more)
  * The decoder uses the shape of the level last given to zc_prepare (5 by default).  zc_autotune times
  * the candidates on a host sample (its whole blocks, up to one encoder launch) and keeps the fastest for
  * (block_log, level); it allocates its own device buffers for the duration of the call. */

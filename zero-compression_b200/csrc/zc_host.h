@@ -71,7 +71,7 @@ struct GraphEntry {
 // the match pass's compare cap and tile (none of them changes a result byte)
 struct Shape {
   uint32_t ring_log = 12, fill_warps = 4, cmp_cap = 16, match_tile = 1024, fill_words = 1, match_dense = 256,
-           match_defer = 2;
+           match_defer = 3;
 };
 
 }  // namespace zch
