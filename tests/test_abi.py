@@ -68,3 +68,34 @@ def test_library_resolves_every_symbol_at_load(so):
     ctypes.CDLL(so, mode=os.RTLD_NOW)
     out = subprocess.run(["nm", "-D", "--undefined-only", so], capture_output=True, text=True).stdout
     assert not re.findall(r"\b_ZN2zc\w+", out)
+
+
+def test_binding_structs_match_the_header(tmp_path):
+    """The ctypes structures of the binding have the header's fields at the header's offsets and sizes,
+    as a C compiler lays them out (gcc on the header itself)."""
+    import zero_cuda as Z
+    structs = {"zc_shape": Z.Shape, "zc_archive_info": Z.ArchiveInfo, "zc_entry": Z._Entry, "zc_job": Z._Job}
+    renamed = {"in_": "in"}  # (a Python keyword in the binding)
+    src = ['#include <stddef.h>', '#include <stdio.h>', f'#include "{os.path.join(INCLUDE, "zero_cuda.h")}"',
+           "int main(void) {"]
+    for cname, py in structs.items():
+        src.append(f'  printf("{cname} (struct) %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            f = renamed.get(fname, fname)
+            src.append(f'  printf("{cname} {fname} %zu %zu\\n", offsetof({cname}, {f}), sizeof((({cname} *)0)->{f}));')
+    src += ["  return 0;", "}"]
+    c = tmp_path / "layout.c"
+    c.write_text("\n".join(src))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-o", str(exe), str(c)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            parts = line.split()
+            got[(parts[0], parts[1])] = tuple(int(x) for x in parts[2:])
+    for cname, py in structs.items():
+        assert got[(cname, "(struct)")] == (ctypes.sizeof(py),), cname
+        for fname, _ in py._fields_:
+            field = getattr(py, fname)
+            assert got[(cname, fname)] == (field.offset, field.size), (cname, fname)
